@@ -1,0 +1,241 @@
+/*
+ * ref_harness.cpp -- runs the reference's OWN kernel bodies and text readers
+ * on the CPU (test infrastructure only; built into oracle/_ref/, never part
+ * of the product).
+ *
+ * Compiled once per variant with -DREF_HI or -DREF_HB and -I pointing at the
+ * reference's source directory, so that
+ *   all_structure_undir.cuh   (read_graphEdges / read_Input_Color / readin_changes)
+ *   gpuFunctions_undir.cuh    (deleteEdgeFromAdj, deleteEdge, insEdge,
+ *                              processChangeEdge, findEligibleNeighbors,
+ *                              recolorNeighbor)
+ * are used unmodified.  The shim in ref_shim/ makes the launch geometry one
+ * thread.  This file re-states only the driver (HI/Color_main.cu:31-247,
+ * HB/Color_main.cu:32-256, HI/supportingFunctions.cu:19-101) with a host
+ * compaction in place of cuCompactor (ascending ids, HI/compactor.cuh:79-173),
+ * and always allocates the frontier buffers (the reference allocates them
+ * only when the batch has deletions, HI/supportingFunctions.cu:69-95).
+ *
+ * Two schedules:
+ *   serial   -- each kernel called once over all its items (index order).
+ *   snapshot -- each kernel item is run alone against a copy of the state at
+ *               the start of the step; the writes of all items are merged
+ *               afterwards (a write conflict aborts).  HB's
+ *               processChangeEdge becomes HB's recolorNeighbor body applied
+ *               to the de-duplicated endpoints of the change list.
+ *
+ * usage: ref_{hi,hb} serial|snapshot graph nodes edges prevColor changes out [iter_cap]
+ * out: "iterations <n> status <0|4>\n" then one colour per line.
+ */
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "gpuFunctions_undir.cuh"
+
+namespace {
+
+struct State {
+  int n = 0;
+  std::vector<int> color, prev, affected;
+  int change = 0;
+};
+
+// Runs one snapshot step: run_item(j) is called for every item against the
+// state as it was when the step began; all writes are merged at the end.
+template <class F>
+bool snapshot_step(State& S, int nitems, F run_item) {
+  const std::vector<int> c0 = S.color, p0 = S.prev, a0 = S.affected;
+  const int ch0 = S.change;
+  std::vector<int> nc = c0, np = p0, na = a0;
+  std::vector<char> wc(S.n, 0), wp(S.n, 0), wa(S.n, 0);
+  int nch = ch0;
+  for (int j = 0; j < nitems; ++j) {
+    S.color = c0;
+    S.prev = p0;
+    S.affected = a0;
+    S.change = ch0;
+    run_item(j);
+    for (int v = 0; v < S.n; ++v) {
+      if (S.color[v] != c0[v]) {
+        if (wc[v] && nc[v] != S.color[v]) return false;
+        wc[v] = 1;
+        nc[v] = S.color[v];
+      }
+      if (S.prev[v] != p0[v]) {
+        if (wp[v] && np[v] != S.prev[v]) return false;
+        wp[v] = 1;
+        np[v] = S.prev[v];
+      }
+      if (S.affected[v] != a0[v]) {
+        if (wa[v] && na[v] != S.affected[v]) return false;
+        wa[v] = 1;
+        na[v] = S.affected[v];
+      }
+    }
+    if (S.change != ch0) nch = S.change;
+  }
+  S.color = nc;
+  S.prev = np;
+  S.affected = na;
+  S.change = nch;
+  return true;
+}
+
+int compact(const State& S, std::vector<int>& list) {
+  int c = 0;
+  for (int v = 0; v < S.n; ++v)
+    if (S.affected[v] == 1) list[c++] = v;
+  return c;
+}
+
+}  // namespace
+
+int main(int argc, char* argv[]) {
+  if (argc < 8) {
+    std::fprintf(stderr,
+                 "usage: %s serial|snapshot graph nodes edges prevColor changes out [iter_cap]\n",
+                 argv[0]);
+    return 2;
+  }
+  const bool snapshot = std::strcmp(argv[1], "snapshot") == 0;
+  const int nodes = std::atoi(argv[3]);
+  const long iter_cap = argc > 8 ? std::atol(argv[8]) : 100000;
+  State S;
+  S.n = nodes;
+  S.color.assign(nodes, 0);
+  S.prev.assign(nodes, -1);  // cudaMemset(previosVertexcolor, -1)
+  S.affected.assign(nodes, 0);
+  std::vector<ColList> AdjList(nodes);
+  int totalInsertion = 0;
+#ifdef REF_HI
+  int maxColor = -1;
+  read_Input_Color(S.color.data(), argv[5], &maxColor);
+  const int W = maxColor / 32 + 2;  // HI/Color_main.cu:69
+  read_graphEdges(AdjList, argv[2]);
+  std::vector<changeEdge> allChange_Ins, allChange_Del;
+  readin_changes(argv[6], allChange_Ins, allChange_Del, AdjList, totalInsertion,
+                 S.color.data());
+#else
+  std::vector<int> prop(nodes, 0);
+  read_Input_Color(S.color.data(), argv[5]);
+  read_graphEdges(AdjList, argv[2], prop.data());
+  std::vector<changeEdge> allChange, allChange_Del;
+  readin_changes(argv[6], allChange, allChange_Del, AdjList, totalInsertion, S.color.data(),
+                 prop.data());
+#endif
+  // CSR flatten, HI/supportingFunctions.cu:27-33
+  std::vector<int> tracker(nodes + 1, 0);
+  std::vector<ColWt> full;
+  for (int i = 0; i < nodes; ++i) {
+    tracker[i + 1] = tracker[i] + (int)AdjList[i].size();
+    full.insert(full.end(), AdjList[i].begin(), AdjList[i].end());
+  }
+  full.push_back(ColWt{0, -1});  // keeps data() valid for an empty graph
+  ColWt* adj = full.data();
+  int* trk = tracker.data();
+  std::vector<int> list(nodes > 0 ? nodes : 1, 0);
+  int counter = 0;
+  int one = 1;
+  bool ok = true;
+
+  if (!allChange_Del.empty())
+    deleteEdgeFromAdj(allChange_Del.data(), (int)allChange_Del.size(), adj, trk);
+
+#ifdef REF_HI
+  if (!allChange_Del.empty()) {
+    if (snapshot) {
+      ok = ok && snapshot_step(S, (int)allChange_Del.size(), [&](int j) {
+        deleteEdge(&allChange_Del[j], S.color.data(), S.prev.data(), 1, adj, trk,
+                   S.affected.data(), &S.change, W);
+      });
+    } else {
+      deleteEdge(allChange_Del.data(), S.color.data(), S.prev.data(), (int)allChange_Del.size(),
+                 adj, trk, S.affected.data(), &S.change, W);
+    }
+  }
+  if (!allChange_Ins.empty()) {
+    if (snapshot) {
+      ok = ok && snapshot_step(S, (int)allChange_Ins.size(), [&](int j) {
+        insEdge(&allChange_Ins[j], S.color.data(), S.prev.data(), 1, adj, trk,
+                S.affected.data(), &S.change, W);
+      });
+    } else {
+      insEdge(allChange_Ins.data(), S.color.data(), S.prev.data(), (int)allChange_Ins.size(), adj,
+              trk, S.affected.data(), &S.change, W);
+    }
+  }
+#else
+  if (snapshot) {
+    std::vector<int> ends;
+    std::vector<char> seen(nodes, 0);
+    for (const changeEdge& c : allChange) {
+      int e[2] = {c.node1, c.node2};
+      for (int x : e)
+        if (!seen[x]) {
+          seen[x] = 1;
+          ends.push_back(x);
+        }
+    }
+    ok = ok && snapshot_step(S, (int)ends.size(), [&](int j) {
+      recolorNeighbor(&ends[j], S.color.data(), adj, trk, S.affected.data(), &one, &S.change,
+                      prop.data());
+    });
+  } else if (!allChange.empty()) {
+    processChangeEdge(allChange.data(), S.color.data(), (int)allChange.size(), adj, trk,
+                      S.affected.data(), &S.change, prop.data());
+  }
+#endif
+
+  long it = 0;
+  int status = 0;
+  counter = compact(S, list);
+  while (ok && S.change > 0) {
+    if (it >= iter_cap) {
+      status = 4;
+      break;
+    }
+    ++it;
+    S.change = 0;
+    std::fill(S.affected.begin(), S.affected.end(), 0);
+#ifdef REF_HI
+    findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.prev.data(), S.color.data(),
+                          &counter);
+#else
+    findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.color.data(), &counter,
+                          prop.data());
+#endif
+    counter = compact(S, list);
+    std::fill(S.affected.begin(), S.affected.end(), 0);
+    if (snapshot) {
+      ok = snapshot_step(S, counter, [&](int j) {
+#ifdef REF_HI
+        recolorNeighbor(&list[j], S.color.data(), S.prev.data(), adj, trk, S.affected.data(), &one,
+                        &S.change, W);
+#else
+        recolorNeighbor(&list[j], S.color.data(), adj, trk, S.affected.data(), &one, &S.change,
+                        prop.data());
+#endif
+      });
+    } else {
+#ifdef REF_HI
+      recolorNeighbor(list.data(), S.color.data(), S.prev.data(), adj, trk, S.affected.data(),
+                      &counter, &S.change, W);
+#else
+      recolorNeighbor(list.data(), S.color.data(), adj, trk, S.affected.data(), &counter,
+                      &S.change, prop.data());
+#endif
+    }
+  }
+  if (!ok) {
+    std::fprintf(stderr, "snapshot write conflict\n");
+    return 3;
+  }
+  FILE* f = std::fopen(argv[7], "w");
+  if (!f) return 2;
+  std::fprintf(f, "iterations %ld status %d\n", it, status);
+  for (int v = 0; v < nodes; ++v) std::fprintf(f, "%d\n", S.color[v]);
+  std::fclose(f);
+  return 0;
+}
