@@ -1,0 +1,756 @@
+// dc_api.cpp -- C ABI of libdyncolor (include/dyncolor.h).
+//
+// Host orchestration only: argument checks, device allocations, the two
+// cooperative launches of a batch (structural update, then seeding +
+// recolouring loop), pool growth and retry, statistics.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/dyncolor.h"
+#include "dc_internal.h"
+
+using namespace dc;
+
+struct dc_ctx {
+  dc_options opt{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sms = 0;
+  int grid_struct = 0;
+  int grid_recolor = 0;
+  std::string err;
+  long long bytes = 0;
+
+  // graph
+  int n = -1;
+  int key_bits = 1;
+  long long pool_cap = 0;
+  long long* off = nullptr;
+  int* len = nullptr;
+  int* cap = nullptr;
+  int* live = nullptr;
+  int* adj = nullptr;
+  int* color = nullptr;
+  int* prev = nullptr;
+  int* prop = nullptr;
+  DevState* st = nullptr;
+  DevState* h_st = nullptr;  // pinned
+  unsigned long long* d_scalar = nullptr;
+  unsigned long long* h_scalar = nullptr;  // pinned
+
+  // recolour scratch (sized by n and pool_cap)
+  long long rc_pool_cap = -1;
+  QueueBufs qb[3]{};
+  unsigned* bmA = nullptr;
+  unsigned* bmB = nullptr;
+  unsigned* bmC = nullptr;
+  int* ncolor = nullptr;
+  int* sat = nullptr;
+
+  // batch scratch (sized by k and pool_cap)
+  long long kcap = 0;
+  long long k_pool_cap = -1;
+  dc_change* d_ch = nullptr;
+  unsigned char* lflag = nullptr;
+  unsigned long long* keysA = nullptr;
+  unsigned long long* keysB = nullptr;
+  unsigned long long* net = nullptr;
+  int* tof = nullptr;
+  unsigned char* present = nullptr;
+  int* rank = nullptr;
+  int* tbeg = nullptr;
+  int* trow = nullptr;
+  int* rowdel = nullptr;
+  int* tins = nullptr;
+  long long* tnoff = nullptr;
+  int* tncap = nullptr;
+  int* tnlive = nullptr;
+  int* trel = nullptr;
+  int* cursor = nullptr;
+  long long* delpos = nullptr;
+  int2* units = nullptr;
+  int2* relunits = nullptr;
+  long long cap_units = 0;
+  long long cap_rel = 0;
+  unsigned* hist = nullptr;
+  unsigned* dscan = nullptr;
+  unsigned* cta_cnt = nullptr;
+
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+dc_status fail(dc_ctx* c, dc_status s, const std::string& what) {
+  if (c) c->err = what;
+  return s;
+}
+
+dc_status cuda_fail(dc_ctx* c, const char* what, cudaError_t e) {
+  return fail(c, e == cudaErrorMemoryAllocation ? DC_E_NOMEM : DC_E_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define DC_CK(call)                                      \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, #call, e_); \
+  } while (0)
+
+template <class T>
+dc_status dalloc(dc_ctx* ctx, T** p, long long count, const char* what) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  if (count <= 0) count = 1;
+  const size_t bytes = (size_t)count * sizeof(T);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(ctx, DC_E_NOMEM, std::string("cudaMalloc ") + what + " (" + std::to_string(bytes) + " bytes)");
+  }
+  ctx->bytes += (long long)bytes;
+  return DC_OK;
+}
+
+template <class T>
+void dfree(dc_ctx* ctx, T** p) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  (void)ctx;
+}
+
+int key_bits_for(int n) {
+  int B = 1;
+  while (B < 31 && (1ll << B) < (long long)n) ++B;
+  return B;
+}
+
+GraphDev graph_dev(const dc_ctx* c) {
+  GraphDev g;
+  g.n = c->n;
+  g.key_bits = c->key_bits;
+  g.off = c->off;
+  g.len = c->len;
+  g.cap = c->cap;
+  g.live = c->live;
+  g.adj = c->adj;
+  g.pool_cap = c->pool_cap;
+  g.color = c->color;
+  g.prev = c->prev;
+  g.prop = c->prop;
+  return g;
+}
+
+int unit_slots(const dc_ctx* c) { return c->opt.unit_slots; }
+
+// Recolour scratch depends on n and on the pool capacity (work units).
+dc_status ensure_recolor_scratch(dc_ctx* ctx) {
+  if (ctx->rc_pool_cap == ctx->pool_cap) return DC_OK;
+  const long long n = std::max(ctx->n, 1);
+  const long long CH = unit_slots(ctx);
+  const long long capU = n + ctx->pool_cap / CH + 64;
+  const long long capM = ctx->pool_cap / CH + 64;
+  const long long words = (n + 31) / 32 + 1;
+  dc_status s;
+  for (int b = 0; b < 3; ++b) {
+    QueueBufs& q = ctx->qb[b];
+    if ((s = dalloc(ctx, &q.itemsA, n, "queue items")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &q.units, capU, "queue units")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &q.gmask, capM * kMaskWords, "queue masks")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &q.gdone, capM, "queue mask counters")) != DC_OK) return s;
+    q.capA = n;
+    q.capU = capU;
+    q.capM = capM;
+  }
+  if (!ctx->bmA) {
+    if ((s = dalloc(ctx, &ctx->bmA, words, "bitmap")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->bmB, words, "bitmap")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->bmC, words, "bitmap")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->ncolor, n, "ncolor")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->sat, n, "sat")) != DC_OK) return s;
+    DC_CK(cudaMemsetAsync(ctx->bmA, 0, words * 4, ctx->stream));
+    DC_CK(cudaMemsetAsync(ctx->bmB, 0, words * 4, ctx->stream));
+    DC_CK(cudaMemsetAsync(ctx->bmC, 0, words * 4, ctx->stream));
+  }
+  ctx->rc_pool_cap = ctx->pool_cap;
+  return DC_OK;
+}
+
+dc_status reset_bitmaps(dc_ctx* ctx) {
+  const long long words = ((long long)std::max(ctx->n, 1) + 31) / 32 + 1;
+  DC_CK(cudaMemsetAsync(ctx->bmA, 0, words * 4, ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->bmB, 0, words * 4, ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->bmC, 0, words * 4, ctx->stream));
+  return DC_OK;
+}
+
+// Batch scratch depends on k (lines) and on the pool capacity (row units).
+dc_status ensure_batch_scratch(dc_ctx* ctx, long long k) {
+  const bool grow_k = k > ctx->kcap;
+  const bool grow_pool = ctx->k_pool_cap != ctx->pool_cap;
+  if (!grow_k && !grow_pool) return DC_OK;
+  dc_status s;
+  const long long G = std::max(ctx->grid_struct, 1);
+  if (grow_k) {
+    const long long kk = std::max<long long>(k, 1024);
+    const long long k2 = 2 * kk;
+    if ((s = dalloc(ctx, &ctx->d_ch, kk, "changes")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->lflag, kk, "line flags")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->keysA, k2, "keys")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->keysB, k2, "keys")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->net, k2, "net")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->tof, k2, "tof")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->present, k2, "present")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->rank, k2, "rank")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->tbeg, k2 + 1, "tbeg")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->trow, k2, "trow")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->rowdel, k2, "rowdel")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->tins, k2, "tins")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->tnoff, k2, "tnoff")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->tncap, k2, "tncap")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->tnlive, k2, "tnlive")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->trel, k2, "trel")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->cursor, k2, "cursor")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->delpos, k2, "delpos")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->hist, G * 256, "hist")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->dscan, G * 256 + 256, "dscan")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &ctx->cta_cnt, G, "cta counts")) != DC_OK) return s;
+    ctx->kcap = kk;
+  }
+  const long long cu = 2 * ctx->kcap + ctx->pool_cap / kStructChunk + 64;
+  if ((s = dalloc(ctx, &ctx->units, cu, "row units")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->relunits, cu, "relocation units")) != DC_OK) return s;
+  ctx->cap_units = cu;
+  ctx->cap_rel = cu;
+  ctx->k_pool_cap = ctx->pool_cap;
+  return DC_OK;
+}
+
+void free_batch_scratch(dc_ctx* ctx) {
+  dfree(ctx, &ctx->d_ch);
+  dfree(ctx, &ctx->lflag);
+  dfree(ctx, &ctx->keysA);
+  dfree(ctx, &ctx->keysB);
+  dfree(ctx, &ctx->net);
+  dfree(ctx, &ctx->tof);
+  dfree(ctx, &ctx->present);
+  dfree(ctx, &ctx->rank);
+  dfree(ctx, &ctx->tbeg);
+  dfree(ctx, &ctx->trow);
+  dfree(ctx, &ctx->rowdel);
+  dfree(ctx, &ctx->tins);
+  dfree(ctx, &ctx->tnoff);
+  dfree(ctx, &ctx->tncap);
+  dfree(ctx, &ctx->tnlive);
+  dfree(ctx, &ctx->trel);
+  dfree(ctx, &ctx->cursor);
+  dfree(ctx, &ctx->delpos);
+  dfree(ctx, &ctx->units);
+  dfree(ctx, &ctx->relunits);
+  dfree(ctx, &ctx->hist);
+  dfree(ctx, &ctx->dscan);
+  dfree(ctx, &ctx->cta_cnt);
+  ctx->kcap = 0;
+  ctx->k_pool_cap = -1;
+}
+
+StructParams struct_params(dc_ctx* ctx, const dc_change* ch, const int* la, const int* lb, long long k) {
+  StructParams p{};
+  p.g = graph_dev(ctx);
+  p.ch = ch;
+  p.la = la;
+  p.lb = lb;
+  p.k = k;
+  p.slack = ctx->opt.slack;
+  p.keysA = ctx->keysA;
+  p.keysB = ctx->keysB;
+  p.hist = ctx->hist;
+  p.dscan = ctx->dscan;
+  p.cta_cnt = ctx->cta_cnt;
+  p.net = ctx->net;
+  p.tof = ctx->tof;
+  p.present = ctx->present;
+  p.rank = ctx->rank;
+  p.tbeg = ctx->tbeg;
+  p.trow = ctx->trow;
+  p.rowdel = ctx->rowdel;
+  p.tins = ctx->tins;
+  p.tnoff = ctx->tnoff;
+  p.tncap = ctx->tncap;
+  p.tnlive = ctx->tnlive;
+  p.trel = ctx->trel;
+  p.cursor = ctx->cursor;
+  p.delpos = ctx->delpos;
+  p.units = ctx->units;
+  p.relunits = ctx->relunits;
+  p.cap_units = ctx->cap_units;
+  p.cap_rel = ctx->cap_rel;
+  p.st = ctx->st;
+  return p;
+}
+
+RecolorParams recolor_params(dc_ctx* ctx, const dc_change* ch, long long k) {
+  RecolorParams p{};
+  p.g = graph_dev(ctx);
+  p.ch = ch;
+  p.k = k;
+  p.variant = ctx->opt.variant;
+  p.unit_slots = unit_slots(ctx);
+  p.iter_cap = ctx->opt.iter_cap;
+  for (int b = 0; b < 3; ++b) p.qb[b] = ctx->qb[b];
+  p.bmA = ctx->bmA;
+  p.bmB = ctx->bmB;
+  p.bmC = ctx->bmC;
+  p.ncolor = ctx->ncolor;
+  p.sat = ctx->sat;
+  p.lflag = ctx->lflag;
+  p.st = ctx->st;
+  return p;
+}
+
+// Clears the per-launch part of DevState and snapshots the pool counter.
+dc_status reset_state(dc_ctx* ctx) {
+  const size_t off = offsetof(DevState, bar_arrived);
+  DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + off, 0, sizeof(DevState) - off, ctx->stream));
+  DC_CK(cudaMemcpyAsync(&ctx->st->pool_used_start, &ctx->st->pool_used, sizeof(unsigned long long),
+                        cudaMemcpyDeviceToDevice, ctx->stream));
+  return DC_OK;
+}
+
+dc_status read_state(dc_ctx* ctx) {
+  DC_CK(cudaMemcpyAsync(ctx->h_st, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+// Moves the adjacency into a fresh pool of new_cap slots (tombstones dropped).
+dc_status repack(dc_ctx* ctx, long long new_cap) {
+  GraphDev g = graph_dev(ctx);
+  long long* off2 = nullptr;
+  int* cap2 = nullptr;
+  int* adj2 = nullptr;
+  long long* scratch = nullptr;
+  const long long n = std::max(ctx->n, 1);
+  dc_status s;
+  if ((s = dalloc(ctx, &off2, n, "repack offsets")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &cap2, n, "repack caps")) != DC_OK) {
+    dfree(ctx, &off2);
+    return s;
+  }
+  if ((s = dalloc(ctx, &adj2, new_cap, "repack pool")) != DC_OK) {
+    dfree(ctx, &off2);
+    dfree(ctx, &cap2);
+    return s;
+  }
+  if ((s = dalloc(ctx, &scratch, n / 256 + 2, "repack scratch")) != DC_OK) {
+    dfree(ctx, &off2);
+    dfree(ctx, &cap2);
+    dfree(ctx, &adj2);
+    return s;
+  }
+  DC_CK(cudaMemsetAsync(&ctx->st->status, 0, sizeof(unsigned), ctx->stream));
+  DC_CK(launch_repack(g, off2, cap2, adj2, new_cap, ctx->opt.slack, &ctx->st->pool_used, &ctx->st->status,
+                      scratch, ctx->stream));
+  if ((s = read_state(ctx)) != DC_OK) return s;
+  dfree(ctx, &scratch);
+  if ((ctx->h_st->status & ST_OVERFLOW) || (long long)ctx->h_st->pool_used > new_cap) {
+    dfree(ctx, &off2);
+    dfree(ctx, &cap2);
+    dfree(ctx, &adj2);
+    return fail(ctx, DC_E_INTERNAL, "repack: pool too small");
+  }
+  dfree(ctx, &ctx->off);
+  dfree(ctx, &ctx->cap);
+  dfree(ctx, &ctx->adj);
+  ctx->off = off2;
+  ctx->cap = cap2;
+  ctx->adj = adj2;
+  ctx->pool_cap = new_cap;
+  return DC_OK;
+}
+
+// Runs one batch (or a load) already resident on the device.
+dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int* lb, long long k,
+                    bool recolor, dc_stats* out) {
+  dc_status s;
+  if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
+  if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+  DC_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  for (int attempt = 0;; ++attempt) {
+    if ((s = reset_state(ctx)) != DC_OK) return s;
+    DC_CK(launch_struct(struct_params(ctx, d_ch, la, lb, k), ctx->grid_struct, ctx->stream));
+    if (recolor) {
+      DC_CK(cudaMemcpyAsync(&ctx->st->pre_status, &ctx->st->status, sizeof(unsigned),
+                            cudaMemcpyDeviceToDevice, ctx->stream));
+      // fresh grid barrier and work counters for the second cooperative launch
+      const size_t b0 = offsetof(DevState, bar_arrived);
+      const size_t b1 = offsetof(DevState, wctr) + sizeof(((DevState*)nullptr)->wctr);
+      DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
+      DC_CK(launch_recolor(recolor_params(ctx, d_ch, k), ctx->grid_recolor, ctx->stream));
+    }
+    DC_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((s = read_state(ctx)) != DC_OK) return s;
+    const unsigned stt = ctx->h_st->status;
+    if ((stt & ST_POOL) && !(stt & (ST_OVERFLOW | ST_TIMEOUT | ST_INVAL)) && attempt < 4) {
+      const long long grow = std::max<long long>(ctx->pool_cap, 4ll * k + 4096);
+      if ((s = repack(ctx, ctx->pool_cap + grow)) != DC_OK) return s;
+      if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
+      if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+      continue;
+    }
+    break;
+  }
+  const DevState& h = *ctx->h_st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  dc_status rc = DC_OK;
+  if (h.status & ST_INVAL)
+    rc = fail(ctx, DC_E_INVAL, "change line with a vertex id outside [0,n) or a self-loop");
+  else if (h.status & ST_TIMEOUT)
+    rc = fail(ctx, DC_E_TIMEOUT, "a device-side grid barrier timed out");
+  else if (h.status & ST_OVERFLOW)
+    rc = fail(ctx, DC_E_INTERNAL, "device-side capacity guard fired");
+  else if (h.status & ST_POOL)
+    rc = fail(ctx, DC_E_NOMEM, "adjacency pool exhausted");
+  else if (h.status & ST_ITER)
+    rc = fail(ctx, DC_E_ITER_LIMIT, "recolour loop reached the iteration cap");
+  if (rc != DC_OK && recolor) {
+    dc_status s2 = reset_bitmaps(ctx);
+    if (s2 != DC_OK) return s2;
+  }
+  if (out) {
+    std::memset(out, 0, sizeof(*out));
+    out->iterations = (int64_t)h.iterations;
+    out->seed_targets = (int64_t)h.seed_targets;
+    out->frontier_total = (int64_t)h.frontier_total;
+    out->slots_scanned = (int64_t)h.slots_scanned;
+    out->edges_inserted = (int64_t)(h.edges_inserted / 2);
+    out->edges_deleted = (int64_t)(h.edges_deleted / 2);
+    out->rows_relocated = (int64_t)h.rows_relocated;
+    out->status = rc;
+    out->max_color = h.cmax;
+    out->device_ms = ms;
+  }
+  return rc;
+}
+
+bool ready(dc_ctx* ctx) { return ctx && ctx->n >= 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char* dc_status_str(dc_status s) {
+  switch (s) {
+    case DC_OK: return "ok";
+    case DC_E_INVAL: return "invalid argument";
+    case DC_E_NOMEM: return "out of memory";
+    case DC_E_CUDA: return "CUDA error";
+    case DC_E_ITER_LIMIT: return "iteration cap reached";
+    case DC_E_STATE: return "call out of order";
+    case DC_E_TIMEOUT: return "device wait timed out";
+    case DC_E_INTERNAL: return "internal capacity guard";
+  }
+  return "unknown";
+}
+
+dc_status dc_options_default(dc_options* opt) {
+  if (!opt) return DC_E_INVAL;
+  std::memset(opt, 0, sizeof(*opt));
+  opt->variant = DC_HI;
+  opt->device = 0;
+  opt->stream = nullptr;
+  opt->iter_cap = 1 << 20;
+  opt->slack = 1.25f;
+  opt->blocks_per_sm = 0;
+  opt->reserve_slots = 0;
+  opt->unit_slots = 4096;
+  return DC_OK;
+}
+
+dc_status dc_create(dc_ctx** out, const dc_options* opt) {
+  if (!out) return DC_E_INVAL;
+  *out = nullptr;
+  dc_options o;
+  if (opt)
+    o = *opt;
+  else
+    dc_options_default(&o);
+  if (o.variant != DC_HI && o.variant != DC_HB) return DC_E_INVAL;
+  if (o.iter_cap <= 0) o.iter_cap = 1 << 20;
+  if (!(o.slack > 1.0f)) o.slack = 1.25f;
+  if (o.unit_slots <= 0) o.unit_slots = 4096;
+  if (o.unit_slots % 128 != 0 || o.unit_slots < 128) return DC_E_INVAL;
+  dc_ctx* ctx = new (std::nothrow) dc_ctx();
+  if (!ctx) return DC_E_NOMEM;
+  ctx->opt = o;
+  ctx->device = o.device;
+  auto bail = [&](dc_status s) {
+    dc_destroy(ctx);
+    return s;
+  };
+  if (cudaSetDevice(o.device) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(DC_E_CUDA);
+  }
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, o.device);
+  cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, o.device);
+  if (!coop || ctx->sms <= 0) return bail(DC_E_CUDA);
+  int occ_s = struct_kernel_occupancy();
+  int occ_r = recolor_kernel_occupancy();
+  if (occ_s <= 0 || occ_r <= 0) return bail(DC_E_CUDA);
+  if (o.blocks_per_sm > 0) {
+    occ_s = std::min(occ_s, o.blocks_per_sm);
+    occ_r = std::min(occ_r, o.blocks_per_sm);
+  }
+  ctx->grid_struct = ctx->sms * occ_s;
+  ctx->grid_recolor = ctx->sms * occ_r;
+  if (o.stream) {
+    ctx->stream = (cudaStream_t)o.stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(DC_E_CUDA);
+    ctx->own_stream = true;
+  }
+  if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+    return bail(DC_E_CUDA);
+  if (cudaMalloc((void**)&ctx->st, sizeof(DevState)) != cudaSuccess) return bail(DC_E_NOMEM);
+  if (cudaMemset(ctx->st, 0, sizeof(DevState)) != cudaSuccess) return bail(DC_E_CUDA);
+  if (cudaMallocHost((void**)&ctx->h_st, sizeof(DevState)) != cudaSuccess) return bail(DC_E_NOMEM);
+  if (cudaMalloc((void**)&ctx->d_scalar, 16) != cudaSuccess) return bail(DC_E_NOMEM);
+  if (cudaMallocHost((void**)&ctx->h_scalar, 16) != cudaSuccess) return bail(DC_E_NOMEM);
+  *out = ctx;
+  return DC_OK;
+}
+
+void dc_destroy(dc_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_batch_scratch(ctx);
+  for (int b = 0; b < 3; ++b) {
+    dfree(ctx, &ctx->qb[b].itemsA);
+    dfree(ctx, &ctx->qb[b].units);
+    dfree(ctx, &ctx->qb[b].gmask);
+    dfree(ctx, &ctx->qb[b].gdone);
+  }
+  dfree(ctx, &ctx->bmA);
+  dfree(ctx, &ctx->bmB);
+  dfree(ctx, &ctx->bmC);
+  dfree(ctx, &ctx->ncolor);
+  dfree(ctx, &ctx->sat);
+  dfree(ctx, &ctx->off);
+  dfree(ctx, &ctx->len);
+  dfree(ctx, &ctx->cap);
+  dfree(ctx, &ctx->live);
+  dfree(ctx, &ctx->adj);
+  dfree(ctx, &ctx->color);
+  dfree(ctx, &ctx->prev);
+  dfree(ctx, &ctx->prop);
+  dfree(ctx, &ctx->st);
+  dfree(ctx, &ctx->d_scalar);
+  if (ctx->h_st) cudaFreeHost(ctx->h_st);
+  if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const int32_t* b, int64_t m) {
+  if (!ctx) return DC_E_INVAL;
+  if (ctx->n >= 0) return fail(ctx, DC_E_STATE, "graph already loaded");
+  if (n < 0 || m < 0 || (m > 0 && (!a || !b))) return fail(ctx, DC_E_INVAL, "bad graph arguments");
+  if (m > (1ll << 30)) return fail(ctx, DC_E_INVAL, "more than 2^30 edge lines");
+  for (int64_t i = 0; i < m; ++i)
+    if (a[i] < 0 || a[i] >= n || b[i] < 0 || b[i] >= n || a[i] == b[i])
+      return fail(ctx, DC_E_INVAL, "edge " + std::to_string(i) + " has an id outside [0,n) or is a self-loop");
+  cudaSetDevice(ctx->device);
+  ctx->n = n;
+  ctx->key_bits = key_bits_for(n);
+  const long long nn = std::max(n, 1);
+  dc_status s;
+  if ((s = dalloc(ctx, &ctx->off, nn, "row offsets")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->len, nn, "row lengths")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->cap, nn, "row capacities")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->live, nn, "row live counts")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->color, nn, "colours")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->prev, nn, "previous colours")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->prop, nn, "degree property")) != DC_OK) return s;
+  DC_CK(cudaMemsetAsync(ctx->off, 0, nn * sizeof(long long), ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->len, 0, nn * sizeof(int), ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->cap, 0, nn * sizeof(int), ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->live, 0, nn * sizeof(int), ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->color, 0, nn * sizeof(int), ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->prev, 0xff, nn * sizeof(int), ctx->stream));  // -1
+  DC_CK(cudaMemsetAsync(ctx->prop, 0, nn * sizeof(int), ctx->stream));
+  const double slack = ctx->opt.slack;
+  long long pool = (long long)std::ceil(2.0 * (double)m * slack) + 8ll * nn + 4096;
+  pool = std::max<long long>(pool, ctx->opt.reserve_slots);
+  ctx->pool_cap = pool;
+  if ((s = dalloc(ctx, &ctx->adj, pool, "adjacency pool")) != DC_OK) return s;
+  DC_CK(cudaMemsetAsync(ctx->st, 0, sizeof(DevState), ctx->stream));
+  if (m > 0) {
+    int* da = nullptr;
+    int* db = nullptr;
+    if ((s = dalloc(ctx, &da, m, "load pairs")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &db, m, "load pairs")) != DC_OK) {
+      dfree(ctx, &da);
+      return s;
+    }
+    cudaMemcpyAsync(da, a, (size_t)m * 4, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(db, b, (size_t)m * 4, cudaMemcpyHostToDevice, ctx->stream);
+    s = run_batch(ctx, nullptr, da, db, m, false, nullptr);
+    dfree(ctx, &da);
+    dfree(ctx, &db);
+    // load-sized scratch is not needed by typical batches
+    free_batch_scratch(ctx);
+    if (s != DC_OK) return s;
+  } else {
+    if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+  }
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (n != ctx->n || (n > 0 && !colors)) return fail(ctx, DC_E_INVAL, "colour array size differs from n");
+  for (int32_t v = 0; v < n; ++v)
+    if (colors[v] < 0) return fail(ctx, DC_E_INVAL, "negative colour at vertex " + std::to_string(v));
+  cudaSetDevice(ctx->device);
+  if (n > 0) DC_CK(cudaMemcpyAsync(ctx->color, colors, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  DC_CK(launch_color_max(graph_dev(ctx), ctx->st, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+dc_status dc_apply_batch(dc_ctx* ctx, const dc_change* changes, int64_t k, dc_stats* out) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (k < 0 || (k > 0 && !changes)) return fail(ctx, DC_E_INVAL, "bad batch arguments");
+  if (k > (1ll << 30)) return fail(ctx, DC_E_INVAL, "more than 2^30 change lines");
+  if (out) std::memset(out, 0, sizeof(*out));
+  if (k == 0) return DC_OK;
+  cudaSetDevice(ctx->device);
+  dc_status s;
+  if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
+  DC_CK(cudaMemcpyAsync(ctx->d_ch, changes, (size_t)k * sizeof(dc_change), cudaMemcpyHostToDevice,
+                        ctx->stream));
+  return run_batch(ctx, ctx->d_ch, nullptr, nullptr, k, true, out);
+}
+
+dc_status dc_apply_batch_device(dc_ctx* ctx, const dc_change* d_changes, int64_t k, dc_stats* out) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (k < 0 || (k > 0 && !d_changes)) return fail(ctx, DC_E_INVAL, "bad batch arguments");
+  if (k > (1ll << 30)) return fail(ctx, DC_E_INVAL, "more than 2^30 change lines");
+  if (out) std::memset(out, 0, sizeof(*out));
+  if (k == 0) return DC_OK;
+  cudaSetDevice(ctx->device);
+  return run_batch(ctx, d_changes, nullptr, nullptr, k, true, out);
+}
+
+dc_status dc_colors_read(dc_ctx* ctx, int32_t* out, int32_t n) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (n != ctx->n || (n > 0 && !out)) return fail(ctx, DC_E_INVAL, "output size differs from n");
+  cudaSetDevice(ctx->device);
+  if (n > 0) DC_CK(cudaMemcpyAsync(out, ctx->color, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+dc_status dc_colors_device(dc_ctx* ctx, int32_t** d_colors) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (!d_colors) return DC_E_INVAL;
+  *d_colors = ctx->color;
+  return DC_OK;
+}
+
+dc_status dc_prop_read(dc_ctx* ctx, int32_t* out, int32_t n) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (n != ctx->n || (n > 0 && !out)) return fail(ctx, DC_E_INVAL, "output size differs from n");
+  cudaSetDevice(ctx->device);
+  if (n > 0) DC_CK(cudaMemcpyAsync(out, ctx->prop, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+dc_status dc_validate(dc_ctx* ctx, int64_t* conflicts) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (!conflicts) return DC_E_INVAL;
+  cudaSetDevice(ctx->device);
+  DC_CK(launch_validate(graph_dev(ctx), ctx->d_scalar, ctx->stream));
+  DC_CK(cudaMemcpyAsync(ctx->h_scalar, ctx->d_scalar, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  *conflicts = (int64_t)ctx->h_scalar[0];
+  return DC_OK;
+}
+
+dc_status dc_neighbors(dc_ctx* ctx, int32_t v, int32_t* out, int32_t cap, int32_t* deg) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (v < 0 || v >= ctx->n || !deg || (cap > 0 && !out)) return fail(ctx, DC_E_INVAL, "bad vertex");
+  cudaSetDevice(ctx->device);
+  long long o = 0;
+  int L = 0;
+  DC_CK(cudaMemcpyAsync(&o, ctx->off + v, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaMemcpyAsync(&L, ctx->len + v, 4, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<int> row((size_t)std::max(L, 1));
+  if (L > 0) {
+    DC_CK(cudaMemcpyAsync(row.data(), ctx->adj + o, (size_t)L * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    DC_CK(cudaStreamSynchronize(ctx->stream));
+  }
+  int d = 0;
+  for (int i = 0; i < L; ++i) {
+    if (row[i] < 0) continue;
+    if (d < cap) out[d] = row[i];
+    ++d;
+  }
+  *deg = d;
+  return DC_OK;
+}
+
+dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (!info) return DC_E_INVAL;
+  cudaSetDevice(ctx->device);
+  DC_CK(launch_count_live(graph_dev(ctx), ctx->d_scalar, ctx->stream));
+  DC_CK(cudaMemcpyAsync(ctx->h_scalar, ctx->d_scalar, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaMemcpyAsync(ctx->h_scalar + 1, &ctx->st->pool_used, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  info->n = ctx->n;
+  info->edges = (int64_t)(ctx->h_scalar[0] / 2);
+  info->slots_used = (int64_t)ctx->h_scalar[1];
+  info->slots_capacity = ctx->pool_cap;
+  info->device_bytes = ctx->bytes;
+  return DC_OK;
+}
+
+dc_status dc_compact(dc_ctx* ctx) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  cudaSetDevice(ctx->device);
+  dc_status s = repack(ctx, ctx->pool_cap);
+  if (s != DC_OK) return s;
+  if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+const char* dc_last_error(const dc_ctx* ctx) {
+  if (!ctx) return "null context";
+  return ctx->err.c_str();
+}
+
+}  // extern "C"

@@ -1,0 +1,161 @@
+// dc_internal.h -- host/device shared layouts of libdyncolor (not part of the
+// public C ABI).  Plain structs of pointers and sizes; no torch types.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/dyncolor.h"
+
+namespace dc {
+
+// Device status bits (DevState::status).
+enum : unsigned {
+  ST_INVAL = 1u << 0,     // a change line is invalid (id out of range / self-loop)
+  ST_POOL = 1u << 1,      // adjacency pool exhausted: host grows it and retries
+  ST_ITER = 1u << 2,      // iteration cap reached
+  ST_TIMEOUT = 1u << 3,   // a grid barrier gave up waiting
+  ST_OVERFLOW = 1u << 4,  // an internal capacity guard fired
+};
+
+constexpr int kThreads = 512;       // threads per CTA of the persistent kernels
+constexpr int kWarps = kThreads / 32;
+constexpr int kSmall = 32;          // rows up to this many slots are "class A" (warp-batched)
+constexpr int kMaskWords = 128;     // colour window per warp: 4096 colours
+constexpr int kMaskBits = kMaskWords * 32;
+constexpr int kStructChunk = 1024;  // slots per unit in the structural row scans
+constexpr int kTomb = -1;           // tombstoned adjacency slot
+constexpr int kNumQueues = 6;       // logical queue counter slots
+constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
+
+// Logical queue counter slots.
+enum { Q_LOOP0 = 0, Q_LOOP1 = 1, Q_LOOP2 = 2, Q_S1 = 3, Q_S2E = 4, Q_S2T = 5 };
+
+struct QCount {
+  unsigned long long countA;  // class A items
+  unsigned long long countU;  // work units (class B/C)
+  unsigned long long masks;   // multi-unit mask slots handed out
+  unsigned long long pad;
+};
+
+// Lives in device memory.  Fields up to `pool_used_start` persist across
+// batches; everything from `bar_arrived` on is cleared before every batch,
+// and bar_arrived .. wctr again before every launch.
+struct DevState {
+  int cmax;                        // upper bound of every colour value
+  int pad0;
+  unsigned long long pool_used;    // adjacency pool slots handed out
+  unsigned long long pool_used_start;
+  // ---- cleared before every kernel launch (bar_arrived .. wctr) ----
+  unsigned bar_arrived;
+  unsigned bar_abort;
+  int chg[2];                      // HB loop: "a colour changed" flags, ring by iteration
+  unsigned long long wctr[3];      // work-grab counters (ring by phase)
+  // ---- cleared before every batch (bar_arrived .. end) ----
+  unsigned status;
+  unsigned pre_status;             // status of the structural launch, copied before the recolour launch
+  // structural kernel
+  unsigned long long nvalid;       // valid change lines
+  unsigned long long nnet;         // netted (row, nbr) entries
+  unsigned long long ntouched;     // touched rows
+  unsigned long long ndel;         // slots to tombstone
+  unsigned long long nunits;       // row-scan units
+  unsigned long long nrel;         // relocation copy units
+  // recolour kernel
+  QCount q[kNumQueues];
+  // statistics
+  unsigned long long iterations;
+  unsigned long long seed_targets;
+  unsigned long long frontier_total;
+  unsigned long long slots_scanned;
+  unsigned long long edges_inserted;  // directed entries (2 per undirected edge)
+  unsigned long long edges_deleted;
+  unsigned long long rows_relocated;
+};
+
+struct GraphDev {
+  int n;
+  int key_bits;          // B with n-1 < 2^B
+  long long* off;        // row start in adj, multiple of 4
+  int* len;              // slots in use (live + tombstones)
+  int* cap;              // slots reserved, multiple of 4
+  int* live;             // live slots
+  int* adj;              // adjacency pool
+  long long pool_cap;
+  int* color;
+  int* prev;             // HI previosVertexcolor
+  int* prop;             // HB vertex_prop
+};
+
+struct QueueBufs {
+  int* itemsA;           // class A items
+  int4* units;           // {vertex, chunk, mask slot, chunks}
+  unsigned* gmask;       // mask slots: kMaskWords words each
+  int* gdone;            // per mask slot: finished units
+  long long capA, capU, capM;
+};
+
+struct StructParams {
+  GraphDev g;
+  const dc_change* ch;   // change lines (update batch) or NULL
+  const int* la;         // graph-load pairs when ch == NULL
+  const int* lb;
+  long long k;           // number of lines
+  float slack;
+  unsigned long long* keysA;  // 2k
+  unsigned long long* keysB;  // 2k
+  unsigned* hist;        // grid * 256
+  unsigned* dscan;       // grid * 256 (digit prefix over CTAs) + 256 totals
+  unsigned* cta_cnt;     // grid
+  unsigned long long* net;    // 2k netted keys
+  int* tof;              // 2k: touched-row index of each net entry
+  unsigned char* present;// 2k
+  int* rank;             // 2k
+  int* tbeg;             // touched rows + 1: first net entry
+  int* trow;             // touched row id
+  int* rowdel;           // per touched row: slots deleted
+  int* tins;             // per touched row: new neighbours
+  long long* tnoff;      // per touched row: new offset
+  int* tncap;
+  int* tnlive;
+  int* trel;
+  int* cursor;
+  long long* delpos;     // absolute slot positions to tombstone
+  int2* units;           // row-scan units {touched row, chunk}
+  int2* relunits;        // relocation copy units
+  long long cap_units;
+  long long cap_rel;
+  DevState* st;
+};
+
+struct RecolorParams {
+  GraphDev g;
+  const dc_change* ch;
+  long long k;
+  int variant;
+  int unit_slots;        // slots per work unit (multiple of 128)
+  long long iter_cap;
+  QueueBufs qb[3];
+  unsigned* bmA;
+  unsigned* bmB;
+  unsigned* bmC;
+  int* ncolor;           // n
+  int* sat;              // n
+  unsigned char* lflag;  // k
+  DevState* st;
+};
+
+// Launchers (dc_struct.cu / dc_recolor.cu / dc_misc.cu).  They return the
+// CUDA error of the launch.
+cudaError_t launch_struct(const StructParams& p, int grid, cudaStream_t s);
+cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s);
+int struct_kernel_occupancy();
+int recolor_kernel_occupancy();
+cudaError_t launch_validate(const GraphDev& g, unsigned long long* out, cudaStream_t s);
+cudaError_t launch_color_max(const GraphDev& g, DevState* st, cudaStream_t s);
+cudaError_t launch_count_live(const GraphDev& g, unsigned long long* out, cudaStream_t s);
+// Repacks rows of g into new arrays (off2/cap2/adj2) with the given slack.
+cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* adj2,
+                          long long cap_slots, float slack, unsigned long long* used,
+                          unsigned* status, long long* scratch, cudaStream_t s);
+
+}  // namespace dc

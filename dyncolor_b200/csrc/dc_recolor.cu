@@ -1,0 +1,700 @@
+// dc_recolor.cu -- seeding + recolouring loop of one update batch, as one
+// cooperative persistent launch with software grid barriers.
+//
+// Snapshot schedule: every reference kernel launch is one step whose reads
+// see the state at the start of the step.  A step that computes colours
+// (REDUCE) writes them to ncolor[]; the following COMMIT step publishes them.
+//
+//   HI  (HI/gpuFunctions_undir.cuh:147-284, HI/Color_main.cu:146-202)
+//     D1  deletions: target = endpoint with the larger colour (tie: node2)
+//     D2  mex of every target                           -> ncolor
+//     D3  commit where the colour changed; frontier F0 += target
+//     I1  insertions whose colours were equal before the batch and still are
+//     I2  saturation size (distinct neighbour colours) of both endpoints
+//     I3  target = endpoint with the smaller saturation (tie: node2)
+//     I4  mex of every target                           -> ncolor
+//     I5  commit unconditionally; F0 += target
+//   HB  (HB/gpuFunctions_undir.cuh:104-314, HB/Color_main.cu:160-224)
+//     H1  every endpoint of (equal-colour insertions + deletions)
+//     H2  mex over neighbours prior in LDF order        -> ncolor
+//     H3  commit where the colour changed; F0 += vertex
+//   loop (both), until the frontier is empty (HI) or nothing changed (HB):
+//     E   findEligibleNeighbors over F  -> next frontier Q (bitmap-deduped)
+//     R   recolorNeighbor's mex over Q  -> ncolor
+//     C   commit Q (HI also saves the previous colour), Q becomes F
+//
+// Work is split by row length: rows of <= kSmall slots ("class A") are
+// processed 32 at a time by one warp with a warp-level load-balanced search
+// over their slots; longer rows become units of up to unit_slots slots, one
+// warp per unit.  A row of several units combines its partial colour masks
+// in a global mask slot; the unit that finishes last computes the result.
+#include "dc_device.cuh"
+
+namespace dc {
+
+namespace {
+
+enum Mode { M_MEX_ALL = 0, M_MEX_PRIOR = 1, M_DISTINCT = 2 };
+
+struct Shared {
+  unsigned mask[kWarps][kMaskWords];  // per-warp colour window
+  long long swll[kWarps];
+};
+
+__device__ __forceinline__ long long grab(unsigned long long* ctr) {
+  unsigned long long x = 0;
+  if (lane_id() == 0) x = atomicAdd(ctr, 1ull);
+  return (long long)__shfl_sync(0xffffffffu, x, 0);
+}
+
+// Pushes u (or nothing when u < 0) into a queue.  All 32 lanes must call.
+__device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const int* len, int u,
+                                          bool allowA, int CH, unsigned* status) {
+  const int L = u >= 0 ? len[u] : 0;
+  const bool isA = u >= 0 && allowA && L <= kSmall;
+  const bool isU = u >= 0 && !isA;
+  const unsigned long long pa = warp_atomic_add(&qc->countA, isA ? 1 : 0);
+  if (isA) {
+    if ((long long)pa < qb.capA)
+      qb.itemsA[pa] = u;
+    else
+      atomicOr(status, ST_OVERFLOW);
+  }
+  int c = 0;
+  if (isU) c = L > CH ? (L + CH - 1) / CH : 1;
+  const unsigned long long pu = warp_atomic_add(&qc->countU, c);
+  if (isU) {
+    int ms = -1;
+    if (c > 1) {
+      ms = (int)atomicAdd(&qc->masks, 1ull);
+      if (ms >= qb.capM) {
+        atomicOr(status, ST_OVERFLOW);
+        return;
+      }
+      uint4* m = reinterpret_cast<uint4*>(qb.gmask + (long long)ms * kMaskWords);
+#pragma unroll 4
+      for (int i = 0; i < kMaskWords / 4; ++i) m[i] = make_uint4(0, 0, 0, 0);
+      qb.gdone[ms] = 0;
+    }
+    for (int q = 0; q < c; ++q) {
+      if ((long long)(pu + q) < qb.capU)
+        qb.units[pu + q] = make_int4(u, q, ms, c);
+      else
+        atomicOr(status, ST_OVERFLOW);
+    }
+  }
+}
+
+// Largest j (0..31) with excl_j <= s, excl held one value per lane and
+// non-decreasing across lanes.  All lanes must call.
+__device__ __forceinline__ int find_owner(int excl, int s) {
+  int j = 0;
+#pragma unroll
+  for (int step = 16; step >= 1; step >>= 1) {
+    const int e = __shfl_sync(0xffffffffu, excl, j + step);
+    if (e <= s) j += step;
+  }
+  return j;
+}
+
+// First zero bit of the window sm[0..nw) (words >= nw count as zero);
+// -1 when all kMaskBits bits are set.  All lanes must call.
+__device__ __forceinline__ int first_zero(const unsigned* sm, int nw) {
+  for (int k0 = 0; k0 < nw; k0 += 32) {
+    const int k = k0 + lane_id();
+    const unsigned word = k < nw ? sm[k] : 0u;
+    const unsigned bal = __ballot_sync(0xffffffffu, word != 0xffffffffu);
+    if (bal) {
+      const int l = __ffs(bal) - 1;
+      const unsigned wd = __shfl_sync(0xffffffffu, word, l);
+      return (k0 + l) * 32 + __ffs(~wd) - 1;
+    }
+  }
+  return nw < kMaskWords ? nw * 32 : -1;
+}
+
+struct Env {
+  struct {
+    unsigned* bmA;
+    unsigned* bmB;
+    unsigned* bmC;
+    int* ncolor;
+  } p;
+  GraphDev g;
+  DevState* st;
+  int variant;
+  int CH;
+  long long my_scanned;
+};
+
+// ---------------------------------------------------------------------
+// slow paths (single warp, whole row): colour windows beyond the first
+// ---------------------------------------------------------------------
+__device__ int slow_mex(Env& E, unsigned* sm, int v, int mode) {
+  const GraphDev& g = E.g;
+  const long long o = g.off[v];
+  const int L = g.len[v];
+  const int pv = mode == M_MEX_PRIOR ? g.prop[v] : 0;
+  for (int w0 = kMaskBits;; w0 += kMaskBits) {
+    for (int k = lane_id(); k < kMaskWords; k += 32) sm[k] = 0;
+    __syncwarp();
+    for (int s0 = 0; s0 < L; s0 += 32) {
+      const int s = s0 + lane_id();
+      if (s < L) {
+        const int u = g.adj[o + s];
+        if (u >= 0 && (mode != M_MEX_PRIOR || is_prior(g.prop[u], u, pv, v))) {
+          const int c = g.color[u] - w0;
+          if (c >= 0 && c < kMaskBits) atomicOr(&sm[c >> 5], 1u << (c & 31));
+        }
+      }
+    }
+    __syncwarp();
+    const int r = first_zero(sm, kMaskWords);
+    __syncwarp();
+    if (r >= 0) return w0 + r;
+    if (w0 > L) return w0;  // unreachable: the mex never exceeds the row length
+  }
+}
+
+__device__ int slow_distinct(Env& E, unsigned* sm, int v, int cmax) {
+  const GraphDev& g = E.g;
+  const long long o = g.off[v];
+  const int L = g.len[v];
+  int total = 0;
+  for (int w0 = kMaskBits; w0 <= cmax; w0 += kMaskBits) {
+    for (int k = lane_id(); k < kMaskWords; k += 32) sm[k] = 0;
+    __syncwarp();
+    for (int s0 = 0; s0 < L; s0 += 32) {
+      const int s = s0 + lane_id();
+      if (s < L) {
+        const int u = g.adj[o + s];
+        if (u >= 0) {
+          const int c = g.color[u] - w0;
+          if (c >= 0 && c < kMaskBits) atomicOr(&sm[c >> 5], 1u << (c & 31));
+        }
+      }
+    }
+    __syncwarp();
+    int cnt = 0;
+    for (int k = lane_id(); k < kMaskWords; k += 32) cnt += __popc(sm[k]);
+    total += (int)warp_sum_ll(cnt);
+    __syncwarp();
+  }
+  return total;
+}
+
+// ---------------------------------------------------------------------
+// REDUCE: colour results of a queue into out[]
+// ---------------------------------------------------------------------
+__device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, int mode, int* out) {
+  const GraphDev& g = E.g;
+  const int v = un.x, chunk = un.y, ms = un.z, nch = un.w;
+  const int L = g.len[v];
+  const long long o = g.off[v];
+  const int s_lo = chunk * E.CH;
+  const int s_hi = min(L, s_lo + E.CH);
+  const int limit = mode == M_DISTINCT ? kMaskBits : min(L, kMaskBits);
+  const int nw = mode == M_DISTINCT ? kMaskWords : min(kMaskWords, (limit + 31) / 32 + 1);
+  unsigned* sm = sh.mask[warp_id()];
+  for (int k = lane_id(); k < nw; k += 32) sm[k] = 0;
+  __syncwarp();
+  const int pv = mode == M_MEX_PRIOR ? g.prop[v] : 0;
+  for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
+    const int s = s0 + lane_id();
+    if (s < s_hi) {
+      const int u = g.adj[o + s];
+      if (u >= 0) {
+        ++E.my_scanned;
+        if (mode != M_MEX_PRIOR || is_prior(g.prop[u], u, pv, v)) {
+          const int c = g.color[u];
+          if (c < limit) atomicOr(&sm[c >> 5], 1u << (c & 31));
+        }
+      }
+    }
+  }
+  __syncwarp();
+  if (nch > 1) {
+    unsigned* gm = qb.gmask + (long long)ms * kMaskWords;
+    for (int k = lane_id(); k < nw; k += 32) {
+      const unsigned x = sm[k];
+      if (x) atomicOr(&gm[k], x);
+    }
+    __threadfence();
+    __syncwarp();
+    int last = 0;
+    if (lane_id() == 0) last = atomicAdd(&qb.gdone[ms], 1) == nch - 1;
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    for (int k = lane_id(); k < nw; k += 32) sm[k] = ld_cg(&gm[k]);
+    __syncwarp();
+  }
+  int r;
+  if (mode == M_DISTINCT) {
+    int cnt = 0;
+    for (int k = lane_id(); k < nw; k += 32) cnt += __popc(sm[k]);
+    r = (int)warp_sum_ll(cnt);
+    __syncwarp();
+    const int cmax = ld_cg(&E.st->cmax);
+    if (cmax >= kMaskBits) r += slow_distinct(E, sm, v, cmax);
+  } else {
+    r = first_zero(sm, nw);
+    __syncwarp();
+    if (r < 0) r = slow_mex(E, sm, v, mode);
+  }
+  if (lane_id() == 0) out[v] = r;
+  __syncwarp();
+}
+
+// Class A batch: 32 rows of <= kSmall slots.  MEX modes only.
+__device__ void reduce_batchA(Env& E, Shared& sh, const QueueBufs& qb, long long cA, long long b,
+                              int mode, int* out) {
+  const GraphDev& g = E.g;
+  const long long idx = b * 32 + lane_id();
+  const bool valid = idx < cA;
+  const int v = valid ? qb.itemsA[idx] : 0;
+  const int L = valid ? g.len[v] : 0;
+  const long long o = valid ? g.off[v] : 0;
+  const int pv = (valid && mode == M_MEX_PRIOR) ? g.prop[v] : 0;
+  unsigned long long* m64 = reinterpret_cast<unsigned long long*>(sh.mask[warp_id()]);
+  m64[lane_id()] = 0ull;
+  __syncwarp();
+  const int incl = warp_incl_scan(L);
+  const int T = __shfl_sync(0xffffffffu, incl, 31);
+  const int excl = incl - L;
+  for (int s0 = 0; s0 < T; s0 += 32) {
+    const int s = s0 + lane_id();
+    const int j = find_owner(excl, s);
+    const int vj = __shfl_sync(0xffffffffu, v, j);
+    const long long oj = __shfl_sync(0xffffffffu, o, j);
+    const int ej = __shfl_sync(0xffffffffu, excl, j);
+    const int pj = __shfl_sync(0xffffffffu, pv, j);
+    if (s < T) {
+      const int u = g.adj[oj + (s - ej)];
+      if (u >= 0) {
+        ++E.my_scanned;
+        if (mode != M_MEX_PRIOR || is_prior(g.prop[u], u, pj, vj)) {
+          const int c = g.color[u];
+          if (c < 64) atomicOr(&m64[j], 1ull << c);
+        }
+      }
+    }
+  }
+  __syncwarp();
+  if (valid) out[v] = __ffsll((long long)~m64[lane_id()]) - 1;
+  __syncwarp();
+}
+
+__device__ void phase_reduce(Env& E, Shared& sh, const QueueBufs& qb, const QCount* qc,
+                             unsigned long long* ctr, int mode, int* out) {
+  const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
+  const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
+  const long long nAb = (cA + 31) / 32;
+  const long long total = cU + nAb;
+  while (true) {
+    const long long i = grab(ctr);
+    if (i >= total) break;
+    if (i < cU)
+      reduce_unit(E, sh, qb, qb.units[i], mode, out);
+    else
+      reduce_batchA(E, sh, qb, cA, i - cU, mode, out);
+  }
+}
+
+// ---------------------------------------------------------------------
+// EXPAND: findEligibleNeighbors of frontier F into queue N (bitmap bmB)
+//   HI: HI/gpuFunctions_undir.cuh:229-260
+//   HB: HB/gpuFunctions_undir.cuh:259-291
+// ---------------------------------------------------------------------
+struct Rule {
+  int v, cv, pv;  // frontier vertex, its colour, prev colour (HI) / prop (HB)
+};
+
+// Decides for one live slot (v -> u) which vertex to mark.
+__device__ __forceinline__ void eligible(const Env& E, const Rule& R, int u, bool* mu, bool* mv) {
+  const int cu = E.g.color[u];
+  if (E.variant == DC_HI) {
+    *mu = (R.cv == cu && R.v < u) || (R.pv < cu);
+    *mv = false;
+  } else {
+    const bool pr = is_prior(R.pv, R.v, E.g.prop[u], u);
+    *mu = pr;
+    *mv = (R.cv == cu) && !pr;
+  }
+}
+
+__device__ __forceinline__ void mark_and_push(Env& E, const QueueBufs& nq, QCount* nc, int u, bool mu,
+                                              int v, bool mv) {
+  const bool cu = mu && mark_bit(E.p.bmB, u);
+  warp_push(nq, nc, E.g.len, cu ? u : -1, true, E.CH, &E.st->status);
+  if (__any_sync(0xffffffffu, mv)) {
+    const bool cv = mv && mark_bit(E.p.bmB, v);
+    warp_push(nq, nc, E.g.len, cv ? v : -1, true, E.CH, &E.st->status);
+  }
+}
+
+__device__ void expand_unit(Env& E, int4 un, const QueueBufs& nq, QCount* nc) {
+  const GraphDev& g = E.g;
+  const int v = un.x;
+  const int L = g.len[v];
+  const long long o = g.off[v];
+  const int s_lo = un.y * E.CH;
+  const int s_hi = min(L, s_lo + E.CH);
+  Rule R;
+  R.v = v;
+  R.cv = g.color[v];
+  R.pv = E.variant == DC_HI ? g.prev[v] : g.prop[v];
+  for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
+    const int s = s0 + lane_id();
+    bool mu = false, mv = false;
+    int u = -1;
+    if (s < s_hi) {
+      u = g.adj[o + s];
+      if (u >= 0) {
+        ++E.my_scanned;
+        eligible(E, R, u, &mu, &mv);
+      }
+    }
+    mark_and_push(E, nq, nc, u, mu, v, mv);
+  }
+}
+
+__device__ void expand_batchA(Env& E, const QueueBufs& fq, long long cA, long long b,
+                              const QueueBufs& nq, QCount* nc) {
+  const GraphDev& g = E.g;
+  const long long idx = b * 32 + lane_id();
+  const bool valid = idx < cA;
+  const int v = valid ? fq.itemsA[idx] : 0;
+  const int L = valid ? g.len[v] : 0;
+  const long long o = valid ? g.off[v] : 0;
+  const int cv = valid ? g.color[v] : 0;
+  const int pv = valid ? (E.variant == DC_HI ? g.prev[v] : g.prop[v]) : 0;
+  const int incl = warp_incl_scan(L);
+  const int T = __shfl_sync(0xffffffffu, incl, 31);
+  const int excl = incl - L;
+  for (int s0 = 0; s0 < T; s0 += 32) {
+    const int s = s0 + lane_id();
+    const int j = find_owner(excl, s);
+    Rule R;
+    R.v = __shfl_sync(0xffffffffu, v, j);
+    R.cv = __shfl_sync(0xffffffffu, cv, j);
+    R.pv = __shfl_sync(0xffffffffu, pv, j);
+    const long long oj = __shfl_sync(0xffffffffu, o, j);
+    const int ej = __shfl_sync(0xffffffffu, excl, j);
+    bool mu = false, mv = false;
+    int u = -1;
+    if (s < T) {
+      u = g.adj[oj + (s - ej)];
+      if (u >= 0) {
+        ++E.my_scanned;
+        eligible(E, R, u, &mu, &mv);
+      }
+    }
+    mark_and_push(E, nq, nc, u, mu, R.v, mv);
+  }
+}
+
+__device__ void phase_expand(Env& E, const QueueBufs& fq, const QCount* fc, const QueueBufs& nq,
+                             QCount* nc, unsigned long long* ctr) {
+  const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
+  const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
+  const long long nAb = (cA + 31) / 32;
+  const long long total = cU + nAb;
+  while (true) {
+    const long long i = grab(ctr);
+    if (i >= total) break;
+    if (i < cU)
+      expand_unit(E, fq.units[i], nq, nc);
+    else
+      expand_batchA(E, fq, cA, i - cU, nq, nc);
+  }
+}
+
+// ---------------------------------------------------------------------
+// COMMIT and line phases
+// ---------------------------------------------------------------------
+enum Commit {
+  C_LOOP = 0,     // prev (HI) and colour from ncolor, clear bmB
+  C_SEED_DEL = 1, // HI deleteEdge: commit if changed, F0 += v, clear bmA
+  C_SEED_INS = 2, // HI insEdge: commit always, F0 += v, clear bmC
+  C_SEED_HB = 3,  // HB processChangeEdge: commit if changed, F0 += v, clear bmA
+  C_CLEAR_A = 4,  // clear bmA only
+  C_CLEAR_B = 5   // clear bmB only
+};
+
+// Item i of a queue: class A items first, then units with chunk 0.
+__device__ __forceinline__ int queue_item(const QueueBufs& qb, long long cA, long long total, long long i) {
+  if (i < cA) return qb.itemsA[i];
+  if (i < total) {
+    const int4 un = qb.units[i - cA];
+    if (un.y == 0) return un.x;
+  }
+  return -1;
+}
+
+__device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int kind,
+                             const QueueBufs* f0, QCount* f0c, long long gwarp, long long nwarps,
+                             unsigned long long* items_stat, int* chg_flag) {
+  const GraphDev& g = E.g;
+  const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
+  const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
+  const long long total = cA + cU;
+  long long items = 0;
+  int cmax_local = -1;
+  bool changed = false;
+  for (long long i0 = gwarp * 32; i0 < total; i0 += nwarps * 32) {
+    const int v = queue_item(qb, cA, total, i0 + lane_id());
+    int push = -1;
+    if (v >= 0) {
+      ++items;
+      switch (kind) {
+        case C_LOOP: {
+          const int nc = ld_cg(&E.p.ncolor[v]);
+          const int oc = g.color[v];
+          if (E.variant == DC_HI) g.prev[v] = oc;
+          if (nc != oc) changed = true;
+          g.color[v] = nc;
+          cmax_local = max(cmax_local, nc);
+          E.p.bmB[v >> 5] = 0u;
+          break;
+        }
+        case C_SEED_DEL:
+        case C_SEED_HB: {
+          const int nc = ld_cg(&E.p.ncolor[v]);
+          const int oc = g.color[v];
+          if (nc != oc) {
+            if (kind == C_SEED_DEL) g.prev[v] = oc;
+            g.color[v] = nc;
+            cmax_local = max(cmax_local, nc);
+            push = v;
+          }
+          E.p.bmA[v >> 5] = 0u;
+          break;
+        }
+        case C_SEED_INS: {
+          const int nc = ld_cg(&E.p.ncolor[v]);
+          g.prev[v] = g.color[v];
+          g.color[v] = nc;
+          cmax_local = max(cmax_local, nc);
+          push = v;
+          E.p.bmC[v >> 5] = 0u;
+          break;
+        }
+        case C_CLEAR_A:
+          E.p.bmA[v >> 5] = 0u;
+          break;
+        default:
+          E.p.bmB[v >> 5] = 0u;
+          break;
+      }
+    }
+    if (f0) {
+      const bool claim = push >= 0 && mark_bit(E.p.bmB, push);
+      warp_push(*f0, f0c, g.len, claim ? push : -1, true, E.CH, &E.st->status);
+    }
+  }
+  const int m = __reduce_max_sync(0xffffffffu, cmax_local);
+  if (lane_id() == 0 && m >= 0) atomicMax(&E.st->cmax, m);
+  const long long it = warp_sum_ll(items);
+  if (lane_id() == 0 && it && items_stat) atomicAdd(items_stat, (unsigned long long)it);
+  if (chg_flag && __any_sync(0xffffffffu, changed) && lane_id() == 0) atomicExch(chg_flag, 1);
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads) recolor_kernel(RecolorParams p) {
+  __shared__ Shared sh;
+  Env E;
+  E.p.bmA = p.bmA;
+  E.p.bmB = p.bmB;
+  E.p.bmC = p.bmC;
+  E.p.ncolor = p.ncolor;
+  E.g = p.g;
+  E.st = p.st;
+  E.variant = p.variant;
+  E.CH = p.unit_slots;
+  E.my_scanned = 0;
+  DevState* st = p.st;
+  const GraphDev& g = E.g;
+  unsigned bar = 0;
+  int ps = 0;  // phase sequence for the work-grab ring
+  const long long gthreads = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  auto ctr = [&]() -> unsigned long long* {
+    if (leader) st->wctr[(ps + 1) % 3] = 0ull;  // next phase's counter (last used 2 phases ago)
+    return &st->wctr[ps % 3];
+  };
+  const QueueBufs& B0 = p.qb[0];  // F0 and even loop queues
+  const QueueBufs& B1 = p.qb[1];  // odd loop queues, HI insertion targets
+  const QueueBufs& B2 = p.qb[2];  // seeding sets
+  const dc_change* ch = p.ch;
+  // The structural launch failed (invalid line, pool exhausted, ...): the
+  // batch is not applied.  Uniform: nothing writes pre_status here.
+  if (ld_cg(&st->pre_status) != 0u) return;
+
+  // ======================= seeding =======================
+  if (p.variant == DC_HI) {
+    // D1: deletion targets (and remember which insertions had equal colours)
+    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+      const long long i = i0 + lane_id();
+      int t = -1;
+      if (i < p.k) {
+        const dc_change c = ch[i];
+        if (c.inst == 0) {
+          t = g.color[c.node1] > g.color[c.node2] ? c.node1 : c.node2;
+        }
+        p.lflag[i] = (c.inst == 1 && g.color[c.node1] == g.color[c.node2]) ? 1 : 0;
+      }
+      const bool claim = t >= 0 && mark_bit(p.bmA, t);
+      warp_push(B2, &st->q[Q_S1], g.len, claim ? t : -1, true, E.CH, &st->status);
+    }
+    if (!grid_sync(st, bar)) return;
+    // D2
+    phase_reduce(E, sh, B2, &st->q[Q_S1], ctr(), M_MEX_ALL, p.ncolor);
+    ++ps;
+    if (!grid_sync(st, bar)) return;
+    // D3
+    phase_commit(E, B2, &st->q[Q_S1], C_SEED_DEL, &B0, &st->q[Q_LOOP0], gwarp, nwarps,
+                 &st->seed_targets, nullptr);
+    if (!grid_sync(st, bar)) return;
+    // I1: insertions still monochromatic -> both endpoints
+    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+      const long long i = i0 + lane_id();
+      int a = -1, b = -1;
+      if (i < p.k && p.lflag[i]) {
+        const dc_change c = ch[i];
+        if (g.color[c.node1] == g.color[c.node2]) {
+          a = c.node1;
+          b = c.node2;
+          p.lflag[i] = 2;
+        }
+      }
+      const bool ca = a >= 0 && mark_bit(p.bmA, a);
+      warp_push(B2, &st->q[Q_S2E], g.len, ca ? a : -1, false, E.CH, &st->status);
+      const bool cb = b >= 0 && mark_bit(p.bmA, b);
+      warp_push(B2, &st->q[Q_S2E], g.len, cb ? b : -1, false, E.CH, &st->status);
+    }
+    if (!grid_sync(st, bar)) return;
+    // I2: saturation sizes
+    phase_reduce(E, sh, B2, &st->q[Q_S2E], ctr(), M_DISTINCT, p.sat);
+    ++ps;
+    if (!grid_sync(st, bar)) return;
+    // I3: targets; release the endpoint set
+    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+      const long long i = i0 + lane_id();
+      int t = -1;
+      if (i < p.k && p.lflag[i] == 2) {
+        const dc_change c = ch[i];
+        t = ld_cg(&p.sat[c.node1]) < ld_cg(&p.sat[c.node2]) ? c.node1 : c.node2;
+      }
+      const bool claim = t >= 0 && mark_bit(p.bmC, t);
+      warp_push(B1, &st->q[Q_S2T], g.len, claim ? t : -1, true, E.CH, &st->status);
+    }
+    phase_commit(E, B2, &st->q[Q_S2E], C_CLEAR_A, nullptr, nullptr, gwarp, nwarps, nullptr,
+                 nullptr);
+    if (!grid_sync(st, bar)) return;
+    // I4
+    phase_reduce(E, sh, B1, &st->q[Q_S2T], ctr(), M_MEX_ALL, p.ncolor);
+    ++ps;
+    if (!grid_sync(st, bar)) return;
+    // I5
+    phase_commit(E, B1, &st->q[Q_S2T], C_SEED_INS, &B0, &st->q[Q_LOOP0], gwarp, nwarps,
+                 &st->seed_targets, nullptr);
+    if (!grid_sync(st, bar)) return;
+  } else {
+    // H1: endpoints of equal-colour insertions and of all deletions
+    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+      const long long i = i0 + lane_id();
+      int a = -1, b = -1;
+      if (i < p.k) {
+        const dc_change c = ch[i];
+        if (c.inst == 0 || (c.inst == 1 && g.color[c.node1] == g.color[c.node2])) {
+          a = c.node1;
+          b = c.node2;
+        }
+      }
+      const bool ca = a >= 0 && mark_bit(p.bmA, a);
+      warp_push(B2, &st->q[Q_S1], g.len, ca ? a : -1, true, E.CH, &st->status);
+      const bool cb = b >= 0 && mark_bit(p.bmA, b);
+      warp_push(B2, &st->q[Q_S1], g.len, cb ? b : -1, true, E.CH, &st->status);
+    }
+    if (!grid_sync(st, bar)) return;
+    // H2
+    phase_reduce(E, sh, B2, &st->q[Q_S1], ctr(), M_MEX_PRIOR, p.ncolor);
+    ++ps;
+    if (!grid_sync(st, bar)) return;
+    // H3
+    phase_commit(E, B2, &st->q[Q_S1], C_SEED_HB, &B0, &st->q[Q_LOOP0], gwarp, nwarps,
+                 &st->seed_targets, nullptr);
+    if (!grid_sync(st, bar)) return;
+  }
+  // F0 is complete: release its marks so the loop can mark into bmB.
+  phase_commit(E, B0, &st->q[Q_LOOP0], C_CLEAR_B, nullptr, nullptr, gwarp, nwarps, nullptr,
+               nullptr);
+  if (!grid_sync(st, bar)) return;
+
+  // ======================= loop =======================
+  {
+    int fs = Q_LOOP0;  // counter slot of the frontier
+    int fb = 0;        // buffer of the frontier
+    const QCount* f0c = &st->q[Q_LOOP0];
+    long long it = 0;
+    const int rmode = p.variant == DC_HI ? M_MEX_ALL : M_MEX_PRIOR;
+    bool go = (ld_cg(&f0c->countA) + ld_cg(&f0c->countU)) > 0;
+    while (go) {
+      if (it >= p.iter_cap) {
+        if (leader) atomicOr(&st->status, ST_ITER);
+        break;
+      }
+      ++it;
+      const int ns = (fs + 1) % 3;
+      const int nb = fb ^ 1;
+      // E
+      if (leader) {
+        QCount* z = &st->q[(fs + 2) % 3];
+        z->countA = 0;
+        z->countU = 0;
+        z->masks = 0;
+      }
+      phase_expand(E, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
+      ++ps;
+      if (!grid_sync(st, bar)) return;
+      const QCount* nc = &st->q[ns];
+      const long long nq = (long long)(ld_cg(&nc->countA) + ld_cg(&nc->countU));
+      if (p.variant == DC_HI && nq == 0) break;
+      // R
+      if (leader) st->chg[(it + 1) & 1] = 0;
+      phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
+      ++ps;
+      if (!grid_sync(st, bar)) return;
+      // C
+      phase_commit(E, p.qb[nb], nc, C_LOOP, nullptr, nullptr, gwarp, nwarps, &st->frontier_total,
+                   &st->chg[it & 1]);
+      if (!grid_sync(st, bar)) return;
+      if (p.variant == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;
+      fs = ns;
+      fb = nb;
+    }
+    if (leader) st->iterations = (unsigned long long)it;
+  }
+  const long long sc = warp_sum_ll(E.my_scanned);
+  if (lane_id() == 0 && sc) atomicAdd(&st->slots_scanned, (unsigned long long)sc);
+}
+
+cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s) {
+  RecolorParams q = p;
+  void* args[] = {&q};
+  return cudaLaunchCooperativeKernel((const void*)recolor_kernel, dim3(grid), dim3(kThreads), args,
+                                     0, s);
+}
+
+int recolor_kernel_occupancy() {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recolor_kernel, kThreads, 0) != cudaSuccess)
+    return 0;
+  return b;
+}
+
+}  // namespace dc

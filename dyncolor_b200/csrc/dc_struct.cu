@@ -1,0 +1,524 @@
+// dc_struct.cu -- structural update of the CSR-with-slack adjacency.
+//
+// One cooperative persistent launch applies a whole batch of change lines
+// (or, in load mode, the initial edge list) to the adjacency:
+//
+//   S0  validate lines, emit two directed keys (row, nbr, op) per line
+//   R*  LSD radix sort of the keys (8-bit digits, stable block ranking)
+//   S1  net every (row, nbr) group: a delete anywhere in the group wins
+//       (the reference appends insertions while reading and tombstones all
+//       copies afterwards, HI/all_structure_undir.cuh:96-110 +
+//       HI/gpuFunctions_undir.cuh:118-142)
+//   S2  touched rows = row starts of the netted list
+//   S3  scan every touched row once; binary-search each live slot in the
+//       row's sorted change list: deletes are recorded, inserts of an
+//       existing neighbour are dropped (the adjacency is a set)
+//   S4  per row: new live count, relocation if capacity is exceeded or the
+//       row is mostly tombstones; pool space from a bump allocator
+//   --  pool check: nothing has been modified yet; on exhaustion the launch
+//       ends with ST_POOL and the host grows the pool and retries
+//   S5  tombstone deletions; LDF degree property +-1 per line
+//       (HB/all_structure_undir.cuh:110-119, 176-178)
+//   S6  relocation copies (dropping tombstones) + appends of new neighbours
+//   S7  row metadata commit
+#include "dc_device.cuh"
+
+namespace dc {
+
+namespace {
+
+constexpr int kIPT = 4;                   // keys per thread per scatter tile
+constexpr int kTile = kThreads * kIPT;
+
+__device__ __forceinline__ void cta_range(long long N, long long* lo, long long* hi) {
+  const long long G = gridDim.x, c = blockIdx.x;
+  *lo = N * c / G;
+  *hi = N * (c + 1) / G;
+}
+
+// Exclusive prefix over CTAs of cta_cnt[] and the grand total.
+__device__ __forceinline__ void cta_prefix(const unsigned* cta_cnt, long long* base,
+                                           long long* total, long long* swll) {
+  long long b = 0, t = 0;
+  for (int c = threadIdx.x; c < (int)gridDim.x; c += blockDim.x) {
+    const long long v = ld_cg(&cta_cnt[c]);
+    t += v;
+    if (c < (int)blockIdx.x) b += v;
+  }
+  *base = block_sum_ll(b, swll);
+  *total = block_sum_ll(t, swll);
+}
+
+__device__ __forceinline__ int warp_atomic_add32(int* ctr, int val) {
+  const int incl = warp_incl_scan(val);
+  const int tot = __shfl_sync(0xffffffffu, incl, 31);
+  int base = 0;
+  if (tot > 0 && lane_id() == 31) base = atomicAdd(ctr, tot);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return base + incl - val;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
+  __shared__ unsigned s_hist[256];
+  __shared__ unsigned s_base[256];
+  __shared__ unsigned s_run[256];
+  __shared__ int s_wc[kWarps][256];
+  __shared__ int s_sw[kWarps + 1];
+  __shared__ long long s_swll[kWarps];
+  __shared__ int s_flag;
+
+  DevState* st = p.st;
+  const GraphDev g = p.g;
+  const int B = g.key_bits;
+  const int tid = threadIdx.x, lane = lane_id(), w = warp_id();
+  const long long gthreads = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + tid;
+  const long long gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const unsigned long long SENT = (1ull << (2 * B + 1)) - 1ull;
+  const long long N = 2 * p.k;
+  unsigned bar = 0;
+
+  // ---------------- S0: keys + validation ----------------
+  {
+    int nv = 0;
+    for (long long i = gtid; i < p.k; i += gthreads) {
+      int a, b, op;
+      if (p.ch) {
+        const dc_change c = p.ch[i];
+        a = c.node1;
+        b = c.node2;
+        op = c.inst;
+      } else {
+        a = p.la[i];
+        b = p.lb[i];
+        op = 1;
+      }
+      unsigned long long k0 = SENT, k1 = SENT;
+      if (op == 0 || op == 1) {
+        if (a < 0 || a >= g.n || b < 0 || b >= g.n || a == b) {
+          atomicOr(&st->status, ST_INVAL);
+        } else {
+          k0 = make_key(a, b, op, B);
+          k1 = make_key(b, a, op, B);
+          ++nv;
+        }
+      }
+      p.keysA[2 * i] = k0;
+      p.keysA[2 * i + 1] = k1;
+    }
+    const long long s = warp_sum_ll(nv);
+    if (lane == 0 && s) atomicAdd(&st->nvalid, (unsigned long long)s);
+  }
+  if (!grid_sync(st, bar)) return;
+  if (ld_cg(&st->status) & ST_INVAL) return;  // nothing modified
+  const long long NV = 2 * (long long)ld_cg(&st->nvalid);
+
+  // ---------------- radix sort of keys[0..N) ----------------
+  unsigned long long* src = p.keysA;
+  unsigned long long* dst = p.keysB;
+  const int nbits = 2 * B + 1;
+  const int passes = (nbits + 7) / 8;
+  const int G = gridDim.x;
+  for (int pass = 0; pass < passes; ++pass) {
+    const int shift = pass * 8;
+    long long lo, hi;
+    cta_range(N, &lo, &hi);
+    // P1: per-CTA digit histogram
+    for (int d = tid; d < 256; d += kThreads) s_hist[d] = 0;
+    __syncthreads();
+    for (long long i = lo + tid; i < hi; i += kThreads)
+      atomicAdd(&s_hist[(unsigned)(src[i] >> shift) & 255u], 1u);
+    __syncthreads();
+    for (int d = tid; d < 256; d += kThreads) p.hist[(long long)blockIdx.x * 256 + d] = s_hist[d];
+    if (!grid_sync(st, bar)) return;
+    // P2: for each digit, exclusive prefix over CTAs
+    for (int d = blockIdx.x; d < 256; d += G) {
+      unsigned run = 0;
+      for (int c0 = 0; c0 < G; c0 += kThreads) {
+        const int c = c0 + tid;
+        const int v = c < G ? (int)ld_cg(&p.hist[(long long)c * 256 + d]) : 0;
+        int tot;
+        const int ex = block_excl_scan(v, s_sw, &tot);
+        if (c < G) p.dscan[(long long)c * 256 + d] = run + ex;
+        run += tot;
+      }
+      if (tid == 0) p.dscan[(long long)G * 256 + d] = run;
+    }
+    if (!grid_sync(st, bar)) return;
+    // P3: stable scatter
+    {
+      const int v = tid < 256 ? (int)ld_cg(&p.dscan[(long long)G * 256 + tid]) : 0;
+      if (tid == 0) s_flag = 0;
+      __syncthreads();
+      if (tid < 256 && (long long)v == N) s_flag = 1;  // every key has this digit
+      int tot;
+      const int ex = block_excl_scan(v, s_sw, &tot);
+      if (tid < 256) {
+        s_base[tid] = (unsigned)ex + ld_cg(&p.dscan[(long long)blockIdx.x * 256 + tid]);
+        s_run[tid] = 0;
+      }
+      for (int i = tid; i < kWarps * 256; i += kThreads) (&s_wc[0][0])[i] = 0;
+      __syncthreads();
+      const bool skip = s_flag != 0;
+      if (!skip) {
+        for (long long tb = lo; tb < hi; tb += kTile) {
+          unsigned long long kk[kIPT];
+          int dd[kIPT], rr[kIPT];
+          const long long wbase = tb + (long long)w * 32 * kIPT;
+#pragma unroll
+          for (int j = 0; j < kIPT; ++j) {
+            const long long idx = wbase + j * 32 + lane;
+            const bool valid = idx < hi;
+            kk[j] = valid ? src[idx] : 0ull;
+            dd[j] = valid ? (int)((kk[j] >> shift) & 255ull) : -1;
+            rr[j] = 0;
+            const unsigned act = __ballot_sync(0xffffffffu, valid);
+            if (valid) {
+              const unsigned peers = __match_any_sync(act, dd[j]);
+              const int leader = __ffs(peers) - 1;
+              const int before = s_wc[w][dd[j]];
+              rr[j] = before + __popc(peers & lanemask_lt());
+              __syncwarp(act);
+              if (lane == leader) s_wc[w][dd[j]] = before + __popc(peers);
+              __syncwarp(act);
+            }
+          }
+          __syncthreads();
+          if (tid < 256) {
+            unsigned run = s_run[tid];
+            for (int ww = 0; ww < kWarps; ++ww) {
+              const int x = s_wc[ww][tid];
+              s_wc[ww][tid] = (int)run;
+              run += (unsigned)x;
+            }
+            s_run[tid] = run;
+          }
+          __syncthreads();
+#pragma unroll
+          for (int j = 0; j < kIPT; ++j)
+            if (dd[j] >= 0) dst[(long long)s_base[dd[j]] + s_wc[w][dd[j]] + rr[j]] = kk[j];
+          __syncthreads();
+          for (int i = tid; i < kWarps * 256; i += kThreads) (&s_wc[0][0])[i] = 0;
+          __syncthreads();
+        }
+      }
+      if (!grid_sync(st, bar)) return;
+      if (!skip) {
+        unsigned long long* t = src;
+        src = dst;
+        dst = t;
+      }
+    }
+  }
+  const unsigned long long* sorted = src;
+
+  // ---------------- S1: net groups (ordered compaction) ----------------
+  {
+    long long lo, hi;
+    cta_range(NV, &lo, &hi);
+    int cnt = 0;
+    for (long long i = lo + tid; i < hi; i += kThreads)
+      cnt += (i == 0) || ((sorted[i] >> 1) != (sorted[i - 1] >> 1));
+    int tot;
+    block_excl_scan(cnt, s_sw, &tot);
+    if (tid == 0) p.cta_cnt[blockIdx.x] = (unsigned)tot;
+    if (!grid_sync(st, bar)) return;
+    long long base, total;
+    cta_prefix(p.cta_cnt, &base, &total, s_swll);
+    if (blockIdx.x == 0 && tid == 0) st->nnet = (unsigned long long)total;
+    long long run = 0;
+    for (long long t0 = lo; t0 < hi; t0 += kThreads) {
+      const long long i = t0 + tid;
+      const int f = (i < hi) && ((i == 0) || ((sorted[i] >> 1) != (sorted[i - 1] >> 1)));
+      int tt;
+      const int ex = block_excl_scan(f, s_sw, &tt);
+      if (f) {
+        const long long j = base + run + ex;
+        p.net[j] = sorted[i];
+        p.present[j] = 0;
+      }
+      run += tt;
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+  const long long NN = (long long)ld_cg(&st->nnet);
+
+  // ---------------- S2: touched rows ----------------
+  {
+    long long lo, hi;
+    cta_range(NN, &lo, &hi);
+    int cnt = 0;
+    for (long long j = lo + tid; j < hi; j += kThreads)
+      cnt += (j == 0) || (key_row(p.net[j], B) != key_row(p.net[j - 1], B));
+    int tot;
+    block_excl_scan(cnt, s_sw, &tot);
+    if (tid == 0) p.cta_cnt[blockIdx.x] = (unsigned)tot;
+    if (!grid_sync(st, bar)) return;
+    long long base, total;
+    cta_prefix(p.cta_cnt, &base, &total, s_swll);
+    if (blockIdx.x == 0 && tid == 0) {
+      st->ntouched = (unsigned long long)total;
+      p.tbeg[total] = (int)NN;
+    }
+    long long run = 0;
+    for (long long t0 = lo; t0 < hi; t0 += kThreads) {
+      const long long j = t0 + tid;
+      const bool in = j < hi;
+      const int f = in && ((j == 0) || (key_row(p.net[j], B) != key_row(p.net[j - 1], B)));
+      int tt;
+      const int ex = block_excl_scan(f, s_sw, &tt);
+      if (in) {
+        const long long t = base + run + ex + f - 1;
+        p.tof[j] = (int)t;
+        if (f) {
+          p.tbeg[t] = (int)j;
+          p.trow[t] = key_row(p.net[j], B);
+        }
+      }
+      run += tt;
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+  const long long NT_ = (long long)ld_cg(&st->ntouched);
+
+  // ---------------- S3a: row-scan units ----------------
+  for (long long t0 = gwarp * 32; t0 < NT_; t0 += nwarps * 32) {
+    const long long t = t0 + lane;
+    int c = 0;
+    if (t < NT_) {
+      const int r = p.trow[t];
+      const int L = g.len[r];
+      p.rowdel[t] = 0;
+      p.tins[t] = 0;
+      p.cursor[t] = 0;
+      c = (L + kStructChunk - 1) / kStructChunk;
+    }
+    const unsigned long long pos = warp_atomic_add(&st->nunits, c);
+    for (int q = 0; q < c; ++q) {
+      if ((long long)(pos + q) < p.cap_units)
+        p.units[pos + q] = make_int2((int)t, q);
+      else
+        atomicOr(&st->status, ST_OVERFLOW);
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+  if (ld_cg(&st->status) & ST_OVERFLOW) return;
+
+  // ---------------- S3b: scan touched rows ----------------
+  {
+    const long long NU = min((long long)ld_cg(&st->nunits), p.cap_units);
+    while (true) {
+      unsigned long long ui = 0;
+      if (lane == 0) ui = atomicAdd(&st->wctr[0], 1ull);
+      ui = __shfl_sync(0xffffffffu, ui, 0);
+      if ((long long)ui >= NU) break;
+      const int2 u = p.units[ui];
+      const int t = u.x;
+      const int r = p.trow[t];
+      const long long o = g.off[r];
+      const int L = g.len[r];
+      const int s_lo = u.y * kStructChunk;
+      const int s_hi = min(L, s_lo + kStructChunk);
+      const int jb = p.tbeg[t], je = p.tbeg[t + 1];
+      int ndel_local = 0;
+      for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
+        const int s = s0 + lane;
+        bool isdel = false;
+        if (s < s_hi) {
+          const int x = g.adj[o + s];
+          if (x >= 0) {
+            int a = jb, b = je;
+            while (a < b) {
+              const int m = (a + b) >> 1;
+              if (key_nbr(p.net[m], B) < x) a = m + 1; else b = m;
+            }
+            if (a < je && key_nbr(p.net[a], B) == x) {
+              if (key_op(p.net[a]) == 0) isdel = true;
+              else p.present[a] = 1;
+            }
+          }
+        }
+        const unsigned long long pos = warp_atomic_add(&st->ndel, isdel ? 1 : 0);
+        if (isdel) {
+          if ((long long)pos < N)
+            p.delpos[pos] = o + s;
+          else
+            atomicOr(&st->status, ST_OVERFLOW);
+          ++ndel_local;
+        }
+      }
+      const long long nd = warp_sum_ll(ndel_local);
+      if (lane == 0 && nd) atomicAdd(&p.rowdel[t], (int)nd);
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+
+  // ---------------- S4a: ranks of new neighbours ----------------
+  for (long long j = gtid; j < NN; j += gthreads) {
+    const unsigned long long kj = p.net[j];
+    if (key_op(kj) == 1 && !p.present[j]) p.rank[j] = atomicAdd(&p.tins[p.tof[j]], 1);
+  }
+  if (!grid_sync(st, bar)) return;
+
+  // ---------------- S4b: per-row capacity decisions ----------------
+  {
+    long long ins = 0, del = 0, rel = 0;
+    for (long long t0 = gwarp * 32; t0 < NT_; t0 += nwarps * 32) {
+      const long long t = t0 + lane;
+      int need = 0, cu = 0;
+      int r = 0, L = 0, C = 0, lv = 0, rd = 0, ti = 0, nl = 0;
+      bool relocate = false;
+      if (t < NT_) {
+        r = p.trow[t];
+        L = g.len[r];
+        C = g.cap[r];
+        lv = g.live[r];
+        rd = p.rowdel[t];
+        ti = p.tins[t];
+        nl = lv - rd + ti;
+        const int tomb = L - lv;
+        relocate = ((long long)L + ti > C) || (tomb > 32 && tomb > lv);
+        if (relocate) {
+          long long want = (long long)ceilf((float)nl * p.slack);
+          if (want < (long long)nl + 4) want = (long long)nl + 4;
+          need = (int)((want + 3) & ~3ll);
+          cu = (L + kStructChunk - 1) / kStructChunk;
+        }
+        ins += ti;
+        del += rd;
+        rel += relocate;
+      }
+      const unsigned long long noff = warp_atomic_add(&st->pool_used, need);
+      const unsigned long long upos = warp_atomic_add(&st->nrel, cu);
+      if (t < NT_) {
+        p.tnlive[t] = nl;
+        p.trel[t] = relocate ? 1 : 0;
+        if (relocate) {
+          p.tnoff[t] = (long long)noff;
+          p.tncap[t] = need;
+          for (int q = 0; q < cu; ++q) {
+            if ((long long)(upos + q) < p.cap_rel)
+              p.relunits[upos + q] = make_int2((int)t, q);
+            else
+              atomicOr(&st->status, ST_OVERFLOW);
+          }
+        } else {
+          p.tnoff[t] = g.off[r];
+          p.tncap[t] = C;
+        }
+      }
+    }
+    ins = warp_sum_ll(ins);
+    del = warp_sum_ll(del);
+    rel = warp_sum_ll(rel);
+    if (lane == 0) {
+      if (ins) atomicAdd(&st->edges_inserted, (unsigned long long)ins);
+      if (del) atomicAdd(&st->edges_deleted, (unsigned long long)del);
+      if (rel) atomicAdd(&st->rows_relocated, (unsigned long long)rel);
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+  {
+    // Uniform decision: every CTA reads the pool counter before anyone
+    // could restore it (the restore happens after one more barrier).
+    const bool fail = (long long)ld_cg(&st->pool_used) > g.pool_cap ||
+                      (ld_cg(&st->status) & ST_OVERFLOW) != 0;
+    if (fail) {
+      if (blockIdx.x == 0 && tid == 0) atomicOr(&st->status, ST_POOL);
+      if (!grid_sync(st, bar)) return;
+      if (blockIdx.x == 0 && tid == 0) st->pool_used = st->pool_used_start;
+      return;
+    }
+  }
+
+  // ---------------- S5: tombstones + degree property ----------------
+  {
+    const long long ND = min((long long)ld_cg(&st->ndel), N);
+    for (long long d = gtid; d < ND; d += gthreads) g.adj[p.delpos[d]] = kTomb;
+    for (long long i = gtid; i < p.k; i += gthreads) {
+      int a, b, op;
+      if (p.ch) {
+        const dc_change c = p.ch[i];
+        a = c.node1;
+        b = c.node2;
+        op = c.inst;
+      } else {
+        a = p.la[i];
+        b = p.lb[i];
+        op = 1;
+      }
+      if (op == 0 || op == 1) {
+        const int dlt = op == 1 ? 1 : -1;
+        atomicAdd(&g.prop[a], dlt);
+        atomicAdd(&g.prop[b], dlt);
+      }
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+
+  // ---------------- S6: relocation copies + appends ----------------
+  {
+    const long long NR = min((long long)ld_cg(&st->nrel), p.cap_rel);
+    while (true) {
+      unsigned long long ui = 0;
+      if (lane == 0) ui = atomicAdd(&st->wctr[1], 1ull);
+      ui = __shfl_sync(0xffffffffu, ui, 0);
+      if ((long long)ui >= NR) break;
+      const int2 u = p.relunits[ui];
+      const int t = u.x;
+      const int r = p.trow[t];
+      const long long o = g.off[r];
+      const int L = g.len[r];
+      const long long no = p.tnoff[t];
+      const int s_lo = u.y * kStructChunk;
+      const int s_hi = min(L, s_lo + kStructChunk);
+      for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
+        const int s = s0 + lane;
+        const int x = s < s_hi ? g.adj[o + s] : kTomb;
+        const int pos = warp_atomic_add32(&p.cursor[t], x >= 0 ? 1 : 0);
+        if (x >= 0) g.adj[no + pos] = x;
+      }
+    }
+    for (long long j = gtid; j < NN; j += gthreads) {
+      const unsigned long long kj = p.net[j];
+      if (key_op(kj) == 1 && !p.present[j]) {
+        const int t = p.tof[j];
+        const int r = p.trow[t];
+        const long long base = p.trel[t] ? (long long)(g.live[r] - p.rowdel[t]) : (long long)g.len[r];
+        g.adj[p.tnoff[t] + base + p.rank[j]] = key_nbr(kj, B);
+      }
+    }
+  }
+  if (!grid_sync(st, bar)) return;
+
+  // ---------------- S7: commit row metadata ----------------
+  for (long long t = gtid; t < NT_; t += gthreads) {
+    const int r = p.trow[t];
+    if (p.trel[t]) {
+      g.off[r] = p.tnoff[t];
+      g.cap[r] = p.tncap[t];
+      g.len[r] = p.tnlive[t];
+    } else {
+      g.len[r] = g.len[r] + p.tins[t];
+    }
+    g.live[r] = p.tnlive[t];
+  }
+}
+
+cudaError_t launch_struct(const StructParams& p, int grid, cudaStream_t s) {
+  StructParams q = p;
+  void* args[] = {&q};
+  return cudaLaunchCooperativeKernel((const void*)struct_kernel, dim3(grid), dim3(kThreads), args,
+                                     0, s);
+}
+
+int struct_kernel_occupancy() {
+  int b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, struct_kernel, kThreads, 0) != cudaSuccess)
+    return 0;
+  return b;
+}
+
+}  // namespace dc

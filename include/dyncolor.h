@@ -1,0 +1,159 @@
+/*
+ * dyncolor.h -- C ABI of the B200 incremental graph-recoloring library
+ * (libdyncolor.so).
+ *
+ * It replaces the host phases of the reference's single-GPU drivers
+ * (DynColorHeuristicIndependent "HI" and DynColorHeuristicBased "HB"):
+ *
+ *   graph-load          read_graphEdges + transfer_data_to_GPU
+ *                       HI/all_structure_undir.cuh:156-183,
+ *                       HB/all_structure_undir.cuh:158-186,
+ *                       HI/supportingFunctions.cu:19-101
+ *   initial-color       read_Input_Color   HI/all_structure_undir.cuh:130-150
+ *   apply-update-batch  readin_changes + deleteEdgeFromAdj + deleteEdge /
+ *                       insEdge (HI) or processChangeEdge (HB) + the
+ *                       findEligibleNeighbors / compact / recolorNeighbor loop
+ *                       HI/all_structure_undir.cuh:78-128,
+ *                       HI/gpuFunctions_undir.cuh:118-284,
+ *                       HB/gpuFunctions_undir.cuh:104-314,
+ *                       HI/Color_main.cu:146-202, HB/Color_main.cu:160-224
+ *   read-colors         the managed vertexcolor array, HI/Color_main.cu:211-216
+ *   validate            validate kernel, HI/gpuFunctions_undir.cuh:289-305
+ *
+ * Semantics.  Every reference kernel launch is one step; all reads of a step
+ * see the state at the start of the step and its writes land at the end
+ * (the reference's kernels race; this library fixes that schedule).  Tie
+ * breaks and rules are the reference's; saturation masks are exact over the
+ * whole colour range.  The adjacency is a set: inserting an existing edge
+ * is a no-op, a deletion removes the edge, and inside one batch every
+ * insertion is applied before every deletion (a delete of the same edge
+ * wins), as in the reference.
+ *
+ * Ownership: host arrays passed in are caller-owned and copied; device state
+ * is library-owned.  A context is used by one host thread at a time.
+ * Every call returns a dc_status; none exits the process.
+ */
+#ifndef DYNCOLOR_H
+#define DYNCOLOR_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DC_OK = 0,
+  DC_E_INVAL = 1,      /* bad argument: id out of range, self-loop, negative colour, ... */
+  DC_E_NOMEM = 2,      /* device or host allocation failed */
+  DC_E_CUDA = 3,       /* a CUDA runtime call failed (see dc_last_error) */
+  DC_E_ITER_LIMIT = 4, /* the recolour loop hit options.iter_cap; colours are partial */
+  DC_E_STATE = 5,      /* call out of order (e.g. apply before load) */
+  DC_E_TIMEOUT = 6,    /* a device-side wait gave up (grid barrier); context unusable */
+  DC_E_INTERNAL = 7    /* a device-side capacity guard fired */
+} dc_status;
+
+typedef enum {
+  DC_HI = 0, /* heuristic-independent: order by colour value */
+  DC_HB = 1  /* heuristic-based: largest-degree-first priority */
+} dc_variant;
+
+/* One change line "node1 node2 weight inst" of the reference's change file
+ * (changeEdge, HI/all_structure_undir.cuh:41-45): inst 1 inserts, inst 0
+ * deletes, any other value is ignored like readin_changes ignores it. */
+typedef struct {
+  int32_t node1;
+  int32_t node2;
+  int32_t inst;
+} dc_change;
+
+typedef struct {
+  int32_t variant;       /* dc_variant */
+  int32_t device;        /* CUDA device ordinal */
+  void* stream;          /* cudaStream_t to run on; NULL: the library creates one */
+  int64_t iter_cap;      /* recolour-loop iteration cap; <= 0: 1<<20 */
+  float slack;           /* row capacity = live * slack when a row is (re)allocated; <= 1: 1.25 */
+  int32_t blocks_per_sm; /* persistent-kernel CTAs per SM; 0: from occupancy */
+  int64_t reserve_slots; /* initial adjacency pool size hint in slots; 0: automatic */
+  int32_t unit_slots;    /* adjacency slots per warp work unit (multiple of 128); 0: 4096 */
+  int32_t reserved[7];
+} dc_options;
+
+typedef struct {
+  int64_t iterations;     /* executions of the recolour loop body */
+  int64_t seed_targets;   /* distinct vertices recomputed by the seeding steps */
+  int64_t frontier_total; /* sum over iterations of the recolour frontier size */
+  int64_t slots_scanned;  /* live adjacency entries read by seeding + loop */
+  int64_t edges_inserted; /* net structural insertions (new edges) */
+  int64_t edges_deleted;  /* net structural deletions (edges removed) */
+  int64_t rows_relocated; /* adjacency rows moved to new capacity */
+  int32_t status;         /* dc_status of the batch */
+  int32_t max_color;      /* an upper bound of every colour after the batch */
+  double device_ms;       /* device time of the batch (CUDA events) */
+} dc_stats;
+
+typedef struct {
+  int32_t n;              /* vertices */
+  int64_t edges;          /* live undirected edges */
+  int64_t slots_used;     /* adjacency pool slots handed out */
+  int64_t slots_capacity; /* adjacency pool capacity in slots */
+  int64_t device_bytes;   /* device memory held by the context */
+} dc_graph_info;
+
+typedef struct dc_ctx dc_ctx;
+
+/* Fills *opt with defaults (variant HI, device 0, library stream). */
+dc_status dc_options_default(dc_options* opt);
+
+/* Creates a context on opt->device. */
+dc_status dc_create(dc_ctx** out, const dc_options* opt);
+void dc_destroy(dc_ctx* ctx);
+
+/* graph-load (read_graphEdges + transfer_data_to_GPU).  Pair i adds the
+ * undirected edge (a[i], b[i]); duplicate pairs collapse; self-loops and ids
+ * outside [0, n) are rejected with DC_E_INVAL before anything changes.  The
+ * HB degree property counts every pair (duplicates too), like
+ * HB/all_structure_undir.cuh:176-178.  Resets colours to 0.  May be called
+ * once per context. */
+dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const int32_t* b,
+                              int64_t m);
+
+/* initial-color (read_Input_Color): colours must be >= 0. */
+dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n);
+
+/* apply-update-batch from host memory (any host pointer; pinned is fastest).
+ * Validates every line first (DC_E_INVAL leaves the state untouched).  Runs
+ * the structural update and the recolouring on the context's stream and
+ * waits for it.  *out (optional) receives the statistics. */
+dc_status dc_apply_batch(dc_ctx* ctx, const dc_change* changes, int64_t k, dc_stats* out);
+
+/* apply-update-batch with the change lines already in device memory. */
+dc_status dc_apply_batch_device(dc_ctx* ctx, const dc_change* d_changes, int64_t k,
+                                dc_stats* out);
+
+/* read-colors into host memory (n = number of vertices). */
+dc_status dc_colors_read(dc_ctx* ctx, int32_t* out, int32_t n);
+/* Device pointer of the colour array (valid until the next load/destroy). */
+dc_status dc_colors_device(dc_ctx* ctx, int32_t** d_colors);
+/* HB degree property, host copy. */
+dc_status dc_prop_read(dc_ctx* ctx, int32_t* out, int32_t n);
+
+/* validate: number of live edges {u,v} with equal colours (0 = proper). */
+dc_status dc_validate(dc_ctx* ctx, int64_t* conflicts);
+
+/* Adjacency of v (live neighbours, any order) into out[cap]; *deg gets the
+ * live degree (may exceed cap). */
+dc_status dc_neighbors(dc_ctx* ctx, int32_t v, int32_t* out, int32_t cap, int32_t* deg);
+
+dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info);
+
+/* Re-packs the adjacency (drops tombstones, re-applies slack). */
+dc_status dc_compact(dc_ctx* ctx);
+
+/* Last error text of the context (never NULL). */
+const char* dc_last_error(const dc_ctx* ctx);
+const char* dc_status_str(dc_status s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

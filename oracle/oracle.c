@@ -264,6 +264,28 @@ int32_t orc_live_degree(const orc_graph* g, int32_t v) {
   return cnt;
 }
 
+static int cmp_i32(const void* x, const void* y) {
+  int32_t a = *(const int32_t*)x, b = *(const int32_t*)y;
+  return (a > b) - (a < b);
+}
+
+int32_t orc_neighbors(const orc_graph* g, int32_t v, int32_t* out, int32_t cap) {
+  int32_t L = g->len[v];
+  int32_t* tmp = (int32_t*)malloc((size_t)(L > 0 ? L : 1) * sizeof(int32_t));
+  int32_t c = 0;
+  for (int32_t i = 0; i < L; ++i)
+    if (g->row[v][i] >= 0) tmp[c++] = g->row[v][i];
+  qsort(tmp, (size_t)c, sizeof(int32_t), cmp_i32);
+  int32_t u = 0;
+  for (int32_t i = 0; i < c; ++i)
+    if (i == 0 || tmp[i] != tmp[i - 1]) {
+      if (u < cap) out[u] = tmp[i];
+      ++u;
+    }
+  free(tmp);
+  return u;
+}
+
 /* validate, HI/gpuFunctions_undir.cuh:289-305 (counted once per u<v slot) */
 int64_t orc_conflicts(const orc_graph* g) {
   int64_t bad = 0;

@@ -88,6 +88,8 @@ int orc_apply_batch(orc_graph* g, int variant, int schedule,
 int64_t orc_conflicts(const orc_graph* g);
 /* number of live distinct neighbours of v (set semantics) */
 int32_t orc_live_degree(const orc_graph* g, int32_t v);
+/* distinct live neighbours of v, ascending, into out[cap]; returns their count */
+int32_t orc_neighbors(const orc_graph* g, int32_t v, int32_t* out, int32_t cap);
 /* 1 if colors[v] == mex{colors[u] : u neighbour of v, u < v} for every v */
 int orc_is_greedy_id_order(const orc_graph* g);
 /* Greedy lowest-free colour in vertex-id order (same rule as above). */

@@ -66,6 +66,8 @@ def lib():
         L.orc_conflicts.argtypes = [P]
         L.orc_live_degree.restype = C.c_int32
         L.orc_live_degree.argtypes = [P, C.c_int32]
+        L.orc_neighbors.restype = C.c_int32
+        L.orc_neighbors.argtypes = [P, C.c_int32, P, C.c_int32]
         L.orc_is_greedy_id_order.argtypes = [P]
         L.orc_greedy_id_order.argtypes = [P]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -132,6 +134,12 @@ class Graph:
 
     def live_degree(self, v: int) -> int:
         return int(lib().orc_live_degree(self._g, v))
+
+    def neighbors(self, v: int) -> np.ndarray:
+        d = lib().orc_neighbors(self._g, int(v), None, 0)
+        out = np.empty(max(d, 1), dtype=np.int32)
+        lib().orc_neighbors(self._g, int(v), _ptr(out), len(out))
+        return out[:d]
 
     def is_greedy_id_order(self) -> bool:
         return lib().orc_is_greedy_id_order(self._g) == 1
