@@ -1,0 +1,470 @@
+#!/usr/bin/env python
+"""Benchmark: edge-updates/s of incremental recolouring on one or more B200s.
+
+Workload (default): undirected R-MAT graph, scale 24 (16.7 M vertices),
+edge factor 16 (a=0.57, b=c=0.19, d=0.05; self-loops and duplicates
+removed, no vertex permutation), greedy lowest-free colouring in vertex-id
+order, then a sequence of update batches of 1,000,000 lines each, 50%
+deletions of existing edges (uniform over edges, so their endpoints follow
+the R-MAT distribution) and 50% insertions of absent pairs with R-MAT
+endpoints.  One step = one batch through apply-update-batch
+(structural update + seeding + recolouring loop).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--variant hi|hb]
+    python bench.py --impl reference ...   # the reference's own code on the CPU
+
+N > 1 runs N independent replicas (the path does not shard a single graph),
+one process per GPU under torch.distributed; value is the sum over replicas
+divided by the slowest replica's device time.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edge-updates/sec"
+UNIT = "edge-updates/s"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--variant", choices=["hi", "hb"], default="hi")
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--edgefactor", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=1_000_000)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=20_000,
+                    help="change lines of the bounded CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-iter-cap", type=int, default=400)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only; no collective on the data path)
+# ---------------------------------------------------------------------------
+
+class Dist:
+    def __init__(self, want_gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as tdist
+
+            torch.cuda.set_device(self.local)
+            tdist.init_process_group("nccl", timeout=datetime.timedelta(minutes=10),
+                                     device_id=torch.device("cuda", self.local))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as tdist
+
+            tdist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as tdist
+
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as tdist
+
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        tdist.all_reduce(t, op=tdist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# workload
+# ---------------------------------------------------------------------------
+
+def workload_dir(args, dist: Dist) -> str:
+    port = os.environ.get("MASTER_PORT", "0")
+    return os.path.join("/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir(),
+                        f"dcbench_{args.scale}_{args.edgefactor}_{args.batch}_{args.seed}_{port}_{os.getppid() if dist.world > 1 else os.getpid()}")
+
+
+def build_workload(args, nbatches: int):
+    import dyncolor_b200 as dc
+
+    n = 1 << args.scale
+    t0 = time.time()
+    a, b = dc.rmat(args.scale, args.edgefactor * n, seed=args.seed)
+    a, b = dc.dedup(n, a, b)
+    colors = dc.greedy_color(n, a, b)
+    es = dc.EdgeSet(n, a, b)
+    half = args.batch // 2
+    batches = [es.sample_batch(half, args.batch - half, mode=dc.INS_RMAT, scale=args.scale,
+                               seed=args.seed * 1000 + i) for i in range(nbatches)]
+    return {"n": n, "a": a, "b": b, "colors": colors, "batches": batches,
+            "gen_s": time.time() - t0}
+
+
+def get_workload(args, dist: Dist, nbatches: int):
+    """Rank 0 builds the workload; other ranks load it from shared memory."""
+    if dist.world == 1:
+        return build_workload(args, nbatches)
+    d = workload_dir(args, dist)
+    if dist.rank == 0:
+        w = build_workload(args, nbatches)
+        os.makedirs(d, exist_ok=True)
+        np.save(os.path.join(d, "a.npy"), w["a"])
+        np.save(os.path.join(d, "b.npy"), w["b"])
+        np.save(os.path.join(d, "colors.npy"), w["colors"])
+        np.save(os.path.join(d, "batches.npy"), np.stack(w["batches"]))
+    dist.barrier()
+    if dist.rank != 0:
+        w = {"n": 1 << args.scale, "a": np.load(os.path.join(d, "a.npy")),
+             "b": np.load(os.path.join(d, "b.npy")), "colors": np.load(os.path.join(d, "colors.npy")),
+             "gen_s": 0.0}
+        w["batches"] = list(np.load(os.path.join(d, "batches.npy")))
+    dist.barrier()
+    if dist.rank == 0:
+        shutil.rmtree(d, ignore_errors=True)
+    return w
+
+
+def config(args, w) -> dict:
+    return {
+        "workload": (f"rmat{args.scale}-ef{args.edgefactor} update batches of {args.batch} lines "
+                     f"(50% deletions of existing edges / 50% insertions of absent R-MAT pairs), "
+                     f"variant {args.variant.upper()}"),
+        "graph": {"vertices": int(w["n"]), "edges": int(len(w["a"])), "generator": "R-MAT a=0.57 b=c=0.19",
+                  "initial_colors": int(w["colors"].max()) + 1, "seed": args.seed},
+        "batch_lines": args.batch,
+        "variant": args.variant.upper(),
+        "l2": "inputs larger than L2 (adjacency >= 2 GB per replica); no flush",
+        "parallelism": "replicas",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if shutil.which("nvidia-smi") is None:
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+             "-lms", "200", "-i", str(self.device)],
+            stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def load_traffic(variant: str):
+    """Per-launch DRAM traffic of the recolour kernel from the committed ncu
+    summary (bytes per scanned adjacency entry), if one exists."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f).get(variant)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baselines (checker code under oracle/, used only here as the baseline)
+# ---------------------------------------------------------------------------
+
+def cpu_baseline_oracle(args, w) -> dict:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    threads = os.cpu_count() or 1
+    po.set_threads(threads)
+    g = po.Graph(w["n"])
+    g.load_edges(w["a"], w["b"])
+    g.set_colors(w["colors"])
+    ch = w["batches"][0][: args.cpu_sample]
+    och = np.empty(len(ch), dtype=po.CHANGE_DTYPE)
+    for f in ("node1", "node2", "inst"):
+        och[f] = ch[f]
+    t0 = time.perf_counter()
+    rc, st = g.apply_batch(och, po.HI if args.variant == "hi" else po.HB, po.SNAPSHOT)
+    dt = time.perf_counter() - t0
+    return {"value": len(och) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"first {len(och)} lines of batch 1 applied to the initial graph by the C "
+                       f"oracle (snapshot schedule, {threads} OpenMP threads): {dt:.2f} s, "
+                       f"{st.iterations} iterations")}
+
+
+def run_reference(args, dist: Dist) -> dict:
+    """The reference's own kernel bodies, run serially on the host (oracle/_ref)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_hi" if args.variant == "hi" else "ref_hb")
+    if not os.path.exists(exe):
+        return {"impl": "reference", "unavailable": "oracle/_ref harness not built (reference sources absent at build time)"}
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+
+    nb = args.warmup + args.steps
+    w = build_workload(args, nb)
+    d = tempfile.mkdtemp()
+    try:
+        np.stack([w["a"], w["b"]], 1).astype(np.int32).tofile(os.path.join(d, "g.bin"))
+        w["colors"].astype(np.int32).tofile(os.path.join(d, "c.bin"))
+        files = []
+        for i in range(nb):
+            f = os.path.join(d, f"x{i}.txt")
+            po.write_change_file(f, w["batches"][i][: args.cpu_sample])
+            files.append(f)
+        out = os.path.join(d, "o.txt")
+        subprocess.run([exe, "bench", os.path.join(d, "g.bin"), str(w["n"]), str(len(w["a"])),
+                        os.path.join(d, "c.bin"), ",".join(files), out, str(args.ref_iter_cap)],
+                       check=True, stdout=subprocess.DEVNULL)
+        rows = [line.split() for line in open(out)]
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    timed = rows[args.warmup:]
+    ms = sum(float(r[5]) for r in timed)
+    its = [int(r[1]) for r in timed]
+    capped = sum(1 for r in timed if r[3] != "0")
+    lines = args.cpu_sample * len(timed)
+    value = lines / (ms / 1e3)
+    sample = (f"first {args.cpu_sample} lines of each of {len(timed)} batches, each applied to the "
+              f"initial graph by the reference's own kernel bodies run serially on 1 host core "
+              f"(iterations {its}, {capped} stopped at the {args.ref_iter_cap}-iteration cap; the "
+              f"reference's 32-bit masks are exact only for colours <= 30)")
+    return {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / len(timed),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": config(args, w),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, dist: Dist):
+    import torch
+
+    import dyncolor_b200 as dc
+
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    K, W = args.steps, args.warmup
+    w = get_workload(args, dist, W + 2 * K)
+    variant = dc.HI if args.variant == "hi" else dc.HB
+    stream = torch.cuda.Stream(device=dev)
+    ctx = dc.Context(variant=variant, device=dev, stream=stream.cuda_stream)
+    t0 = time.time()
+    ctx.load_edges(w["n"], w["a"], w["b"])
+    ctx.set_colors(w["colors"])
+    load_s = time.time() - t0
+    k = args.batch
+    # device-resident inputs for the kernel-time measurement
+    dbat = [torch.from_numpy(np.ascontiguousarray(x).view(np.int32).reshape(-1, 3)).to(f"cuda:{dev}")
+            for x in w["batches"][: W + K]]
+    torch.cuda.synchronize()
+    for i in range(W):
+        ctx.apply_batch_device(dbat[i].data_ptr(), k)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0.record(stream)
+    stats = []
+    for i in range(K):
+        stats.append(ctx.apply_batch_device(dbat[W + i].data_ptr(), k))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms_local = e0.elapsed_time(e1)
+    ms = dist.max(ms_local)
+    total_updates = dist.sum(float(K * k))
+    value = total_updates / (ms / 1e3)
+    # end to end: pinned host lines in, full colour array out, every step
+    host = [torch.from_numpy(np.ascontiguousarray(x).view(np.int32).reshape(-1)).pin_memory()
+            for x in w["batches"][W + K: W + 2 * K]]
+    colors_out = torch.empty(w["n"], dtype=torch.int32).pin_memory()
+    cnp = colors_out.numpy()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for i in range(K):
+        ctx.apply_batch(host[i].numpy().view(dc.CHANGE_DTYPE))
+        ctx.colors(out=cnp)
+    torch.cuda.synchronize()
+    e2e_s = dist.max(time.perf_counter() - t0)
+    conflicts = ctx.validate()
+    del dbat
+    # roofline of the dominant kernel
+    rec_ms = sum(s.recolor_ms for s in stats)
+    str_ms = sum(s.struct_ms for s in stats)
+    scanned = sum(s.slots_scanned for s in stats)
+    per_slot = 8 if variant == dc.HI else 12  # adjacency id + neighbour colour (+ priority)
+    peak, peak_kind = hbm_peak()
+    if rec_ms >= str_ms:
+        dom, dom_ms, alg = "recolor_kernel", rec_ms, per_slot * scanned
+    else:
+        dom, dom_ms = "struct_kernel", str_ms
+        alg = 16 * 2 * k * K
+    achieved = alg / (dom_ms / 1e3) / 1e9
+    traffic = None
+    tr = load_traffic(args.variant)
+    if tr and dom == "recolor_kernel":
+        traffic = tr["dram_bytes_per_slot"] * scanned / K
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": dist.world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int32",
+        "data": "synthetic",
+        "config": config(args, w),
+        "e2e": {"value": total_updates / e2e_s if e2e_s > 0 else None, "unit": UNIT,
+                "h2d_bytes_per_step": 12 * k, "d2h_bytes_per_step": 4 * int(w["n"])},
+        "gpu_launches": 2 * K,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg / K,
+                     "note": f"{per_slot} B per scanned adjacency entry (id + neighbour colour"
+                             + (" + priority" if variant == dc.HB else "") + ")"},
+        "clocks": clk,
+        "detail": {
+            "iterations_per_batch": [int(s.iterations) for s in stats],
+            "struct_ms_per_batch": str_ms / K,
+            "recolor_ms_per_batch": rec_ms / K,
+            "slots_scanned_per_batch": scanned / K,
+            "max_color": int(max(s.max_color for s in stats)),
+            "conflicts_after": int(conflicts),
+            "workload_gen_s": round(w["gen_s"], 1),
+            "load_s": round(load_s, 2),
+        },
+    }
+    ctx.close()
+    return out, w
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        # the reference has no GPU path here: rank 0 times it, other ranks exit
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(run_reference(args, _Solo(args.gpus))),
+                  flush=True)
+        return
+    dist = Dist(args.gpus)
+    try:
+        out, w = run_ours(args, dist)
+        if dist.rank == 0:
+            if dist.world == 1 and not args.no_cpu_baseline:
+                out["cpu_baseline"] = cpu_baseline_oracle(args, w)
+            print(json.dumps(out), flush=True)
+    finally:
+        dist.close()
+
+
+class _Solo:
+    """World description for the reference arm (no process group)."""
+
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", str(max(gpus, 1))))
+        self.rank = 0
+
+
+if __name__ == "__main__":
+    main()

@@ -64,6 +64,8 @@ class Stats(C.Structure):
         ("status", C.c_int32),
         ("max_color", C.c_int32),
         ("device_ms", C.c_double),
+        ("struct_ms", C.c_double),
+        ("recolor_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -84,7 +84,7 @@ struct dc_ctx {
   unsigned* dscan = nullptr;
   unsigned* cta_cnt = nullptr;
 
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
 };
 
 namespace {
@@ -392,6 +392,7 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   for (int attempt = 0;; ++attempt) {
     if ((s = reset_state(ctx)) != DC_OK) return s;
     DC_CK(launch_struct(struct_params(ctx, d_ch, la, lb, k), ctx->grid_struct, ctx->stream));
+    DC_CK(cudaEventRecord(ctx->evm, ctx->stream));
     if (recolor) {
       DC_CK(cudaMemcpyAsync(&ctx->st->pre_status, &ctx->st->status, sizeof(unsigned),
                             cudaMemcpyDeviceToDevice, ctx->stream));
@@ -414,8 +415,10 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
     break;
   }
   const DevState& h = *ctx->h_st;
-  float ms = 0.f;
+  float ms = 0.f, ms_s = 0.f, ms_r = 0.f;
   cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  cudaEventElapsedTime(&ms_s, ctx->ev0, ctx->evm);
+  cudaEventElapsedTime(&ms_r, ctx->evm, ctx->ev1);
   dc_status rc = DC_OK;
   if (h.status & ST_INVAL)
     rc = fail(ctx, DC_E_INVAL, "change line with a vertex id outside [0,n) or a self-loop");
@@ -443,6 +446,8 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
     out->status = rc;
     out->max_color = h.cmax;
     out->device_ms = ms;
+    out->struct_ms = ms_s;
+    out->recolor_ms = ms_r;
   }
   return rc;
 }
@@ -525,7 +530,8 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(DC_E_CUDA);
     ctx->own_stream = true;
   }
-  if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+  if (cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+      cudaEventCreate(&ctx->evm) != cudaSuccess)
     return bail(DC_E_CUDA);
   if (cudaMalloc((void**)&ctx->st, sizeof(DevState)) != cudaSuccess) return bail(DC_E_NOMEM);
   if (cudaMemset(ctx->st, 0, sizeof(DevState)) != cudaSuccess) return bail(DC_E_CUDA);
@@ -566,6 +572,7 @@ void dc_destroy(dc_ctx* ctx) {
   if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->evm) cudaEventDestroy(ctx->evm);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

@@ -352,31 +352,52 @@ int64_t dcg_edgeset_sample_batch(dcg_edgeset* s, int64_t k_del, int64_t k_ins, i
   }
   const RmatThresholds t = rmat_thresholds(a, b, c);
   const uint64_t n = (uint64_t)s->n;
-  int64_t tries = 0;
-  for (int64_t q = 0; q < k_ins;) {
-    if (++tries > 1000 * (k_ins + 16)) return -DC_E_INVAL;  // graph too dense for the request
-    uint64_t u = 0, v = 0;
-    if (ins_mode == DCG_INS_RMAT) {
-      rmat_pair(x, scale, t, u, v);
-      u %= n;
-      v %= n;
-    } else if (ins_mode == DCG_INS_DEGREE && E > 0) {
-      const uint64_t i = uniform_below(x, E);
-      u = (splitmix64(x) & 1) ? (s->e0[i] >> 32) : (s->e0[i] & 0xffffffffull);
-      v = uniform_below(x, n);
-    } else {
-      u = uniform_below(x, n);
-      v = uniform_below(x, n);
+  // Candidates are drawn and membership-checked in parallel (one random
+  // stream per candidate index), then accepted in index order, so the
+  // result does not depend on the thread count.
+  const uint64_t round_seed = splitmix64(x);
+  int64_t need = k_ins, drawn = 0;
+  std::vector<uint64_t> cand;
+  std::vector<uint8_t> ok;
+  while (need > 0) {
+    if (drawn > 1000 * (k_ins + 16)) return -DC_E_INVAL;  // graph too dense for the request
+    const int64_t C = need + need / 8 + 64;
+    cand.assign((size_t)C, 0);
+    ok.assign((size_t)C, 0);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+      uint64_t y = stream_seed(round_seed, (uint64_t)(drawn + i));
+      uint64_t u = 0, v = 0;
+      if (ins_mode == DCG_INS_RMAT) {
+        rmat_pair(y, scale, t, u, v);
+        u %= n;
+        v %= n;
+      } else if (ins_mode == DCG_INS_DEGREE && E > 0) {
+        const uint64_t j = uniform_below(y, E);
+        u = (splitmix64(y) & 1) ? (s->e0[j] >> 32) : (s->e0[j] & 0xffffffffull);
+        v = uniform_below(y, n);
+      } else {
+        u = uniform_below(y, n);
+        v = uniform_below(y, n);
+      }
+      if (u == v) continue;
+      const uint64_t k = pair_key((int32_t)u, (int32_t)v);
+      cand[(size_t)i] = k;
+      ok[(size_t)i] = !s->present(k);
     }
-    if (u == v) continue;
-    const uint64_t k = pair_key((int32_t)u, (int32_t)v);
-    if (s->present(k) || deleted_now.contains(k)) continue;
-    s->ins.insert(k);
-    out[w].node1 = (int32_t)u;
-    out[w].node2 = (int32_t)v;
-    out[w].inst = 1;
-    ++w;
-    ++q;
+    drawn += C;
+    for (int64_t i = 0; i < C && need > 0; ++i) {
+      if (!ok[(size_t)i]) continue;
+      const uint64_t k = cand[(size_t)i];
+      if (deleted_now.contains(k) || !s->ins.insert(k)) continue;
+      // randomise which endpoint is node1
+      const bool flip = (k ^ (k >> 29)) & 1;
+      out[w].node1 = (int32_t)(flip ? (k & 0xffffffffull) : (k >> 32));
+      out[w].node2 = (int32_t)(flip ? (k >> 32) : (k & 0xffffffffull));
+      out[w].inst = 1;
+      ++w;
+      --need;
+    }
   }
   for (int64_t i = w - 1; i > 0; --i) {
     const int64_t j = (int64_t)uniform_below(x, (uint64_t)i + 1);

@@ -89,6 +89,8 @@ typedef struct {
   int32_t status;         /* dc_status of the batch */
   int32_t max_color;      /* an upper bound of every colour after the batch */
   double device_ms;       /* device time of the batch (CUDA events) */
+  double struct_ms;       /* of which the structural-update launch */
+  double recolor_ms;      /* of which the seeding + recolour launch */
 } dc_stats;
 
 typedef struct {

@@ -26,10 +26,24 @@
  *
  * usage: ref_{hi,hb} serial|snapshot graph nodes edges prevColor changes out [iter_cap]
  * out: "iterations <n> status <0|4>\n" then one colour per line.
+ *
+ * Timing mode (serial schedule, for the CPU baseline of the benchmark):
+ *   ref_{hi,hb} bench graph.bin nodes edges colors.bin ch1[,ch2,...] out [iter_cap]
+ * graph.bin holds int32 pairs (a0 b0 a1 b1 ...) turned into the adjacency the
+ * way read_graphEdges does; colors.bin holds one int32 per vertex.  Every
+ * change file is one step applied to the initial graph and colouring (the
+ * state is restored between steps, untimed).  The timed region of a step is
+ * readin_changes + deleteEdgeFromAdj + seeding + loop (the CSR flatten
+ * between them is not timed); out gets one line per step:
+ * "iterations <n> status <s> time_ms <t>".
  */
+#include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
+#include <utility>
 #include <vector>
 
 #include "gpuFunctions_undir.cuh"
@@ -92,47 +106,57 @@ int compact(const State& S, std::vector<int>& list) {
 
 }  // namespace
 
-int main(int argc, char* argv[]) {
-  if (argc < 8) {
-    std::fprintf(stderr,
-                 "usage: %s serial|snapshot graph nodes edges prevColor changes out [iter_cap]\n",
-                 argv[0]);
-    return 2;
-  }
-  const bool snapshot = std::strcmp(argv[1], "snapshot") == 0;
-  const int nodes = std::atoi(argv[3]);
-  const long iter_cap = argc > 8 ? std::atol(argv[8]) : 100000;
-  State S;
-  S.n = nodes;
-  S.color.assign(nodes, 0);
-  S.prev.assign(nodes, -1);  // cudaMemset(previosVertexcolor, -1)
-  S.affected.assign(nodes, 0);
-  std::vector<ColList> AdjList(nodes);
+namespace {
+
+struct Graph {
+  int nodes = 0;
+  std::vector<ColList> adj;
+#ifndef REF_HI
+  std::vector<int> prop;
+#endif
+};
+
+struct StepResult {
+  long iterations = 0;
+  int status = 0;
+  double ms = 0;
+  bool ok = true;
+};
+
+// One update batch as the reference driver applies it
+// (HI/Color_main.cu:62-202, HB/Color_main.cu:71-224).
+StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long iter_cap) {
+  using clk = std::chrono::steady_clock;
+  StepResult R;
+  const int nodes = G.nodes;
   int totalInsertion = 0;
 #ifdef REF_HI
   int maxColor = -1;
-  read_Input_Color(S.color.data(), argv[5], &maxColor);
+  for (int v = 0; v < nodes; ++v) maxColor = std::max(maxColor, S.color[v]);
   const int W = maxColor / 32 + 2;  // HI/Color_main.cu:69
-  read_graphEdges(AdjList, argv[2]);
   std::vector<changeEdge> allChange_Ins, allChange_Del;
-  readin_changes(argv[6], allChange_Ins, allChange_Del, AdjList, totalInsertion,
+  clk::time_point t0 = clk::now();
+  readin_changes(const_cast<char*>(changes), allChange_Ins, allChange_Del, G.adj, totalInsertion,
                  S.color.data());
 #else
-  std::vector<int> prop(nodes, 0);
-  read_Input_Color(S.color.data(), argv[5]);
-  read_graphEdges(AdjList, argv[2], prop.data());
   std::vector<changeEdge> allChange, allChange_Del;
-  readin_changes(argv[6], allChange, allChange_Del, AdjList, totalInsertion, S.color.data(),
-                 prop.data());
+  clk::time_point t0 = clk::now();
+  readin_changes(const_cast<char*>(changes), allChange, allChange_Del, G.adj, totalInsertion,
+                 S.color.data(), G.prop.data());
 #endif
-  // CSR flatten, HI/supportingFunctions.cu:27-33
+  R.ms += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  // CSR flatten, HI/supportingFunctions.cu:27-33 (not timed)
   std::vector<int> tracker(nodes + 1, 0);
   std::vector<ColWt> full;
+  size_t total = 0;
+  for (int i = 0; i < nodes; ++i) total += G.adj[i].size();
+  full.reserve(total + 1);
   for (int i = 0; i < nodes; ++i) {
-    tracker[i + 1] = tracker[i] + (int)AdjList[i].size();
-    full.insert(full.end(), AdjList[i].begin(), AdjList[i].end());
+    tracker[i + 1] = tracker[i] + (int)G.adj[i].size();
+    full.insert(full.end(), G.adj[i].begin(), G.adj[i].end());
   }
   full.push_back(ColWt{0, -1});  // keeps data() valid for an empty graph
+  t0 = clk::now();
   ColWt* adj = full.data();
   int* trk = tracker.data();
   std::vector<int> list(nodes > 0 ? nodes : 1, 0);
@@ -167,6 +191,7 @@ int main(int argc, char* argv[]) {
     }
   }
 #else
+  int* prop = G.prop.data();
   if (snapshot) {
     std::vector<int> ends;
     std::vector<char> seen(nodes, 0);
@@ -180,20 +205,19 @@ int main(int argc, char* argv[]) {
     }
     ok = ok && snapshot_step(S, (int)ends.size(), [&](int j) {
       recolorNeighbor(&ends[j], S.color.data(), adj, trk, S.affected.data(), &one, &S.change,
-                      prop.data());
+                      prop);
     });
   } else if (!allChange.empty()) {
     processChangeEdge(allChange.data(), S.color.data(), (int)allChange.size(), adj, trk,
-                      S.affected.data(), &S.change, prop.data());
+                      S.affected.data(), &S.change, prop);
   }
 #endif
 
   long it = 0;
-  int status = 0;
   counter = compact(S, list);
   while (ok && S.change > 0) {
     if (it >= iter_cap) {
-      status = 4;
+      R.status = 4;
       break;
     }
     ++it;
@@ -204,7 +228,7 @@ int main(int argc, char* argv[]) {
                           &counter);
 #else
     findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.color.data(), &counter,
-                          prop.data());
+                          prop);
 #endif
     counter = compact(S, list);
     std::fill(S.affected.begin(), S.affected.end(), 0);
@@ -215,7 +239,7 @@ int main(int argc, char* argv[]) {
                         &S.change, W);
 #else
         recolorNeighbor(&list[j], S.color.data(), adj, trk, S.affected.data(), &one, &S.change,
-                        prop.data());
+                        prop);
 #endif
       });
     } else {
@@ -224,18 +248,117 @@ int main(int argc, char* argv[]) {
                       &counter, &S.change, W);
 #else
       recolorNeighbor(list.data(), S.color.data(), adj, trk, S.affected.data(), &counter,
-                      &S.change, prop.data());
+                      &S.change, prop);
 #endif
     }
   }
-  if (!ok) {
-    std::fprintf(stderr, "snapshot write conflict\n");
-    return 3;
+  R.ms += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
+  R.iterations = it;
+  R.ok = ok;
+  return R;
+}
+
+}  // namespace
+
+int main(int argc, char* argv[]) {
+  if (argc < 8) {
+    std::fprintf(stderr,
+                 "usage: %s serial|snapshot|bench graph nodes edges prevColor changes out [iter_cap]\n",
+                 argv[0]);
+    return 2;
+  }
+  const bool bench = std::strcmp(argv[1], "bench") == 0;
+  const bool snapshot = std::strcmp(argv[1], "snapshot") == 0;
+  const int nodes = std::atoi(argv[3]);
+  const long iter_cap = argc > 8 ? std::atol(argv[8]) : 100000;
+  Graph G;
+  G.nodes = nodes;
+  G.adj.resize(nodes);
+  State S;
+  S.n = nodes;
+  S.color.assign(nodes, 0);
+  S.prev.assign(nodes, -1);  // cudaMemset(previosVertexcolor, -1)
+  S.affected.assign(nodes, 0);
+#ifndef REF_HI
+  G.prop.assign(nodes, 0);
+#endif
+  if (bench) {
+    // binary inputs, same adjacency as read_graphEdges builds
+    FILE* fg = std::fopen(argv[2], "rb");
+    FILE* fc = std::fopen(argv[5], "rb");
+    if (!fg || !fc) return 2;
+    std::vector<int> pair(2 * 65536);
+    size_t got;
+    while ((got = std::fread(pair.data(), sizeof(int), pair.size(), fg)) >= 2) {
+      for (size_t i = 0; i + 1 < got; i += 2) {
+        const int n1 = pair[i], n2 = pair[i + 1];
+        G.adj[n2].push_back(ColWt{n1, 0});
+        G.adj[n1].push_back(ColWt{n2, 0});
+#ifndef REF_HI
+        G.prop[n1] += 1;
+        G.prop[n2] += 1;
+#endif
+      }
+    }
+    std::fclose(fg);
+    if (std::fread(S.color.data(), sizeof(int), nodes, fc) != (size_t)nodes) return 2;
+    std::fclose(fc);
+  } else {
+#ifdef REF_HI
+    int maxColor = -1;
+    read_Input_Color(S.color.data(), argv[5], &maxColor);
+    read_graphEdges(G.adj, argv[2]);
+#else
+    read_Input_Color(S.color.data(), argv[5]);
+    read_graphEdges(G.adj, argv[2], G.prop.data());
+#endif
   }
   FILE* f = std::fopen(argv[7], "w");
   if (!f) return 2;
-  std::fprintf(f, "iterations %ld status %d\n", it, status);
-  for (int v = 0; v < nodes; ++v) std::fprintf(f, "%d\n", S.color[v]);
+  if (!bench) {
+    const StepResult R = run_step(G, S, argv[6], snapshot, iter_cap);
+    if (!R.ok) {
+      std::fprintf(stderr, "snapshot write conflict\n");
+      std::fclose(f);
+      return 3;
+    }
+    std::fprintf(f, "iterations %ld status %d\n", R.iterations, R.status);
+    for (int v = 0; v < nodes; ++v) std::fprintf(f, "%d\n", S.color[v]);
+    std::fclose(f);
+    return 0;
+  }
+  // bench: every comma-separated change file is one step on the initial state
+  const State S0 = S;
+#ifndef REF_HI
+  const std::vector<int> prop0 = G.prop;
+#endif
+  std::string list = argv[6];
+  size_t pos = 0;
+  while (pos <= list.size()) {
+    size_t comma = list.find(',', pos);
+    if (comma == std::string::npos) comma = list.size();
+    const std::string file = list.substr(pos, comma - pos);
+    pos = comma + 1;
+    if (file.empty()) continue;
+    // rows an insertion may grow: every vertex named by the file
+    std::vector<std::pair<int, size_t>> sizes;
+    if (FILE* cf = std::fopen(file.c_str(), "r")) {
+      int x, y, w, t;
+      while (std::fscanf(cf, "%d %d %d %d", &x, &y, &w, &t) == 4) {
+        if (x >= 0 && x < nodes) sizes.emplace_back(x, G.adj[x].size());
+        if (y >= 0 && y < nodes) sizes.emplace_back(y, G.adj[y].size());
+      }
+      std::fclose(cf);
+    }
+    const StepResult R = run_step(G, S, file.c_str(), false, iter_cap);
+    std::fprintf(f, "iterations %ld status %d time_ms %.3f\n", R.iterations, R.status, R.ms);
+    std::fflush(f);
+    for (auto it = sizes.rbegin(); it != sizes.rend(); ++it) G.adj[it->first].resize(it->second);
+    S = S0;
+#ifndef REF_HI
+    G.prop = prop0;
+#endif
+  }
   std::fclose(f);
   return 0;
 }
