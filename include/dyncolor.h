@@ -151,6 +151,28 @@ dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info);
 /* Re-packs the adjacency (drops tombstones, re-applies slack). */
 dc_status dc_compact(dc_ctx* ctx);
 
+/* Colouring check that allocates no device or host memory (no counterpart
+ * in the reference).  For callers that cannot let a library call
+ * cudaMalloc: a serving process whose device memory is fully budgeted, an
+ * application whose own allocator owns every device byte, or code that must
+ * avoid the device synchronisation cudaMalloc/cudaFree can cause.  Checks
+ * the colouring of a CSR the caller holds in device memory (row r has
+ * d_row_len[r] entries from d_adj[d_row_off[r]]; negative entries are
+ * skipped as deleted) on the current device and `stream`, and returns the
+ * number of monochromatic edges {u,v}, of vertices on such an edge, and the
+ * largest colour.  n must not exceed 16,777,216 (2^24): the scratch bitmap
+ * is a fixed 2 MiB device array inside the library, held by every GPU that
+ * loads it until the process exits.  The first call on a device looks that
+ * array up (cudaGetSymbolAddress), so make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (other streams,
+ * other host threads) race.  Synchronises `stream` before returning.
+ * DC_E_INVAL: n out of range, a negative colour or a neighbour id outside
+ * [0, n). */
+dc_status dc_validate_csr_noalloc(int32_t n, const int64_t* d_row_off, const int32_t* d_row_len,
+                                  const int32_t* d_adj, const int32_t* d_colors, void* stream,
+                                  int64_t* conflicts, int64_t* conflicted_vertices,
+                                  int32_t* max_color);
+
 /* Last error text of the context (never NULL). */
 const char* dc_last_error(const dc_ctx* ctx);
 const char* dc_status_str(dc_status s);
