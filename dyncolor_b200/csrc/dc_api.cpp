@@ -162,15 +162,18 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
   const long long n = std::max(ctx->n, 1);
   const long long CH = unit_slots(ctx);
   const long long capU = n + ctx->pool_cap / CH + 64;
-  const long long capM = ctx->pool_cap / CH + 64;
+  // mask words: a multi-unit row (length L > CH) takes at most L/32 + 7
+  // words in the mex modes and 132 words for saturation sizes (buffer 2)
+  const long long capM_mex = ctx->pool_cap / 32 + 8 * (ctx->pool_cap / CH) + 1024;
+  const long long capM_dist = std::max(capM_mex, 132 * (ctx->pool_cap / CH) + 1024);
   const long long words = (n + 31) / 32 + 1;
   dc_status s;
   for (int b = 0; b < 3; ++b) {
     QueueBufs& q = ctx->qb[b];
     if ((s = dalloc(ctx, &q.itemsA, n, "queue items")) != DC_OK) return s;
     if ((s = dalloc(ctx, &q.units, capU, "queue units")) != DC_OK) return s;
-    if ((s = dalloc(ctx, &q.gmask, capM * kMaskWords, "queue masks")) != DC_OK) return s;
-    if ((s = dalloc(ctx, &q.gdone, capM, "queue mask counters")) != DC_OK) return s;
+    const long long capM = b == 2 ? capM_dist : capM_mex;
+    if ((s = dalloc(ctx, &q.gmask, capM, "queue masks")) != DC_OK) return s;
     q.capA = n;
     q.capU = capU;
     q.capM = capM;
@@ -482,7 +485,7 @@ dc_status dc_options_default(dc_options* opt) {
   opt->slack = 1.25f;
   opt->blocks_per_sm = 0;
   opt->reserve_slots = 0;
-  opt->unit_slots = 4096;
+  opt->unit_slots = kUnitSlotsDefault;
   return DC_OK;
 }
 
@@ -497,7 +500,7 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   if (o.variant != DC_HI && o.variant != DC_HB) return DC_E_INVAL;
   if (o.iter_cap <= 0) o.iter_cap = 1 << 20;
   if (!(o.slack > 1.0f)) o.slack = 1.25f;
-  if (o.unit_slots <= 0) o.unit_slots = 4096;
+  if (o.unit_slots <= 0) o.unit_slots = kUnitSlotsDefault;
   if (o.unit_slots % 128 != 0 || o.unit_slots < 128) return DC_E_INVAL;
   dc_ctx* ctx = new (std::nothrow) dc_ctx();
   if (!ctx) return DC_E_NOMEM;
@@ -551,7 +554,6 @@ void dc_destroy(dc_ctx* ctx) {
     dfree(ctx, &ctx->qb[b].itemsA);
     dfree(ctx, &ctx->qb[b].units);
     dfree(ctx, &ctx->qb[b].gmask);
-    dfree(ctx, &ctx->qb[b].gdone);
   }
   dfree(ctx, &ctx->bmA);
   dfree(ctx, &ctx->bmB);

@@ -25,6 +25,7 @@ constexpr int kMaskBits = kMaskWords * 32;
 constexpr int kStructChunk = 1024;  // slots per unit in the structural row scans
 constexpr int kTomb = -1;           // tombstoned adjacency slot
 constexpr int kNumQueues = 6;       // logical queue counter slots
+constexpr int kUnitSlotsDefault = 2048;  // adjacency slots per warp work unit
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
 
 // Logical queue counter slots.
@@ -33,7 +34,7 @@ enum { Q_LOOP0 = 0, Q_LOOP1 = 1, Q_LOOP2 = 2, Q_S1 = 3, Q_S2E = 4, Q_S2T = 5 };
 struct QCount {
   unsigned long long countA;  // class A items
   unsigned long long countU;  // work units (class B/C)
-  unsigned long long masks;   // multi-unit mask slots handed out
+  unsigned long long masks;   // multi-unit mask words handed out
   unsigned long long pad;
 };
 
@@ -88,10 +89,9 @@ struct GraphDev {
 
 struct QueueBufs {
   int* itemsA;           // class A items
-  int4* units;           // {vertex, chunk, mask slot, chunks}
-  unsigned* gmask;       // mask slots: kMaskWords words each
-  int* gdone;            // per mask slot: finished units
-  long long capA, capU, capM;
+  int4* units;           // {vertex, chunk, mask word offset, chunks}
+  unsigned* gmask;       // per multi-unit row: [done counter, mask words...], 4-word aligned
+  long long capA, capU, capM;  // capM in 32-bit words
 };
 
 struct StructParams {

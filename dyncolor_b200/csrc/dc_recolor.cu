@@ -47,9 +47,21 @@ __device__ __forceinline__ long long grab(unsigned long long* ctr) {
   return (long long)__shfl_sync(0xffffffffu, x, 0);
 }
 
-// Pushes u (or nothing when u < 0) into a queue.  All 32 lanes must call.
+// Mask words a row of L slots needs in a colour window: the mex of at most
+// L colours is at most L, so colours >= min(L, kMaskBits) never matter;
+// saturation sizes need the whole window.  At least 2 words (colours < 64
+// are folded in from per-lane registers).
+__device__ __forceinline__ int mask_words(int L, int mode) {
+  if (mode == M_DISTINCT) return kMaskWords;
+  const int limit = min(L, kMaskBits);
+  return min(kMaskWords, max(2, (limit + 31) / 32 + 1));
+}
+
+// Pushes u (or nothing when u < 0) into a queue.  Rows of more than one
+// unit get a global mask region [done counter, mask words...].  All 32 lanes
+// must call.
 __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const int* len, int u,
-                                          bool allowA, int CH, unsigned* status) {
+                                          bool allowA, int mode, int CH, unsigned* status) {
   const int L = u >= 0 ? len[u] : 0;
   const bool isA = u >= 0 && allowA && L <= kSmall;
   const bool isU = u >= 0 && !isA;
@@ -66,15 +78,15 @@ __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const
   if (isU) {
     int ms = -1;
     if (c > 1) {
-      ms = (int)atomicAdd(&qc->masks, 1ull);
-      if (ms >= qb.capM) {
+      const int words = (mask_words(L, mode) + 1 + 3) & ~3;
+      const unsigned long long mo = atomicAdd(&qc->masks, (unsigned long long)words);
+      if ((long long)(mo + words) > qb.capM) {
         atomicOr(status, ST_OVERFLOW);
         return;
       }
-      uint4* m = reinterpret_cast<uint4*>(qb.gmask + (long long)ms * kMaskWords);
-#pragma unroll 4
-      for (int i = 0; i < kMaskWords / 4; ++i) m[i] = make_uint4(0, 0, 0, 0);
-      qb.gdone[ms] = 0;
+      uint4* m = reinterpret_cast<uint4*>(qb.gmask + mo);
+      for (int i = 0; i < words / 4; ++i) m[i] = make_uint4(0, 0, 0, 0);
+      ms = (int)mo;
     }
     for (int q = 0; q < c; ++q) {
       if ((long long)(pu + q) < qb.capU)
@@ -186,6 +198,18 @@ __device__ int slow_distinct(Env& E, unsigned* sm, int v, int cmax) {
 // ---------------------------------------------------------------------
 // REDUCE: colour results of a queue into out[]
 // ---------------------------------------------------------------------
+// Folds per-lane masks of colours < 64 into words 0 and 1 of the window.
+__device__ __forceinline__ void fold_low(unsigned* sm, unsigned long long lm) {
+  const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)lm);
+  const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(lm >> 32));
+  __syncwarp();
+  if (lane_id() == 0) {
+    sm[0] |= lo;
+    sm[1] |= hi;
+  }
+  __syncwarp();
+}
+
 __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, int mode, int* out) {
   const GraphDev& g = E.g;
   const int v = un.x, chunk = un.y, ms = un.z, nch = un.w;
@@ -194,39 +218,57 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
   const int s_lo = chunk * E.CH;
   const int s_hi = min(L, s_lo + E.CH);
   const int limit = mode == M_DISTINCT ? kMaskBits : min(L, kMaskBits);
-  const int nw = mode == M_DISTINCT ? kMaskWords : min(kMaskWords, (limit + 31) / 32 + 1);
+  const int nw = mask_words(L, mode);
   unsigned* sm = sh.mask[warp_id()];
   for (int k = lane_id(); k < nw; k += 32) sm[k] = 0;
   __syncwarp();
   const int pv = mode == M_MEX_PRIOR ? g.prop[v] : 0;
-  for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
-    const int s = s0 + lane_id();
-    if (s < s_hi) {
-      const int u = g.adj[o + s];
-      if (u >= 0) {
-        ++E.my_scanned;
-        if (mode != M_MEX_PRIOR || is_prior(g.prop[u], u, pv, v)) {
-          const int c = g.color[u];
-          if (c < limit) atomicOr(&sm[c >> 5], 1u << (c & 31));
-        }
-      }
+  unsigned long long lm = 0;  // colours < 64 seen by this lane
+  // Four slots per lane per round: one aligned 16-byte load (rows start on
+  // 4-slot boundaries and hold capacity up to a multiple of 4) and four
+  // independent colour gathers in flight.
+  for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
+    const int base = r0 + lane_id() * 4;
+    int4 q = make_int4(-1, -1, -1, -1);
+    if (base < s_hi) q = __ldg(reinterpret_cast<const int4*>(g.adj + o + base));
+    const int uu[4] = {q.x, q.y, q.z, q.w};
+    bool ok[4];
+    int cc[4], pp[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ok[j] = base + j < s_hi && uu[j] >= 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? g.color[uu[j]] : 0;
+    if (mode == M_MEX_PRIOR) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) pp[j] = ok[j] ? g.prop[uu[j]] : 0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (!ok[j]) continue;
+      ++E.my_scanned;
+      if (mode == M_MEX_PRIOR && !is_prior(pp[j], uu[j], pv, v)) continue;
+      const int c = cc[j];
+      if (c < 64)
+        lm |= 1ull << c;
+      else if (c < limit)
+        atomicOr(&sm[c >> 5], 1u << (c & 31));
     }
   }
-  __syncwarp();
+  fold_low(sm, lm);
   if (nch > 1) {
-    unsigned* gm = qb.gmask + (long long)ms * kMaskWords;
+    unsigned* gm = qb.gmask + ms;  // [0]: finished units, [1..nw]: mask
     for (int k = lane_id(); k < nw; k += 32) {
       const unsigned x = sm[k];
-      if (x) atomicOr(&gm[k], x);
+      if (x) atomicOr(&gm[1 + k], x);
     }
     __threadfence();
     __syncwarp();
     int last = 0;
-    if (lane_id() == 0) last = atomicAdd(&qb.gdone[ms], 1) == nch - 1;
+    if (lane_id() == 0) last = atomicAdd(&gm[0], 1u) == (unsigned)(nch - 1);
     last = __shfl_sync(0xffffffffu, last, 0);
     if (!last) return;
     __threadfence();
-    for (int k = lane_id(); k < nw; k += 32) sm[k] = ld_cg(&gm[k]);
+    for (int k = lane_id(); k < nw; k += 32) sm[k] = ld_cg(&gm[1 + k]);
     __syncwarp();
   }
   int r;
@@ -246,7 +288,9 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
   __syncwarp();
 }
 
-// Class A batch: 32 rows of <= kSmall slots.  MEX modes only.
+// Class A batch: 32 rows of <= kSmall slots.  MEX modes only.  Each lane
+// handles four slots per round (a warp-level load-balanced search finds the
+// row of every slot) so four gathers are in flight.
 __device__ void reduce_batchA(Env& E, Shared& sh, const QueueBufs& qb, long long cA, long long b,
                               int mode, int* out) {
   const GraphDev& g = E.g;
@@ -262,22 +306,30 @@ __device__ void reduce_batchA(Env& E, Shared& sh, const QueueBufs& qb, long long
   const int incl = warp_incl_scan(L);
   const int T = __shfl_sync(0xffffffffu, incl, 31);
   const int excl = incl - L;
-  for (int s0 = 0; s0 < T; s0 += 32) {
-    const int s = s0 + lane_id();
-    const int j = find_owner(excl, s);
-    const int vj = __shfl_sync(0xffffffffu, v, j);
-    const long long oj = __shfl_sync(0xffffffffu, o, j);
-    const int ej = __shfl_sync(0xffffffffu, excl, j);
-    const int pj = __shfl_sync(0xffffffffu, pv, j);
-    if (s < T) {
-      const int u = g.adj[oj + (s - ej)];
-      if (u >= 0) {
-        ++E.my_scanned;
-        if (mode != M_MEX_PRIOR || is_prior(g.prop[u], u, pj, vj)) {
-          const int c = g.color[u];
-          if (c < 64) atomicOr(&m64[j], 1ull << c);
-        }
-      }
+  for (int s0 = 0; s0 < T; s0 += 128) {
+    int jj[4], vj[4], pj[4], uu[4], cc[4], pp[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int s = s0 + r * 32 + lane_id();
+      jj[r] = find_owner(excl, s);
+      vj[r] = __shfl_sync(0xffffffffu, v, jj[r]);
+      const long long oj = __shfl_sync(0xffffffffu, o, jj[r]);
+      const int ej = __shfl_sync(0xffffffffu, excl, jj[r]);
+      pj[r] = __shfl_sync(0xffffffffu, pv, jj[r]);
+      uu[r] = s < T ? g.adj[oj + (s - ej)] : -1;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? g.color[uu[r]] : 0;
+    if (mode == M_MEX_PRIOR) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) pp[r] = uu[r] >= 0 ? g.prop[uu[r]] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (uu[r] < 0) continue;
+      ++E.my_scanned;
+      if (mode == M_MEX_PRIOR && !is_prior(pp[r], uu[r], pj[r], vj[r])) continue;
+      if (cc[r] < 64) atomicOr(&m64[jj[r]], 1ull << cc[r]);
     }
   }
   __syncwarp();
@@ -310,27 +362,24 @@ struct Rule {
   int v, cv, pv;  // frontier vertex, its colour, prev colour (HI) / prop (HB)
 };
 
-// Decides for one live slot (v -> u) which vertex to mark.
-__device__ __forceinline__ void eligible(const Env& E, const Rule& R, int u, bool* mu, bool* mv) {
-  const int cu = E.g.color[u];
+// Decides for one live slot (v -> u) which vertex to mark, given u's colour
+// cu and (HB) degree property pu.
+__device__ __forceinline__ void eligible(const Env& E, const Rule& R, int u, int cu, int pu, bool* mu,
+                                         bool* mv) {
   if (E.variant == DC_HI) {
     *mu = (R.cv == cu && R.v < u) || (R.pv < cu);
     *mv = false;
   } else {
-    const bool pr = is_prior(R.pv, R.v, E.g.prop[u], u);
+    const bool pr = is_prior(R.pv, R.v, pu, u);
     *mu = pr;
     *mv = (R.cv == cu) && !pr;
   }
 }
 
-__device__ __forceinline__ void mark_and_push(Env& E, const QueueBufs& nq, QCount* nc, int u, bool mu,
-                                              int v, bool mv) {
-  const bool cu = mu && mark_bit(E.p.bmB, u);
-  warp_push(nq, nc, E.g.len, cu ? u : -1, true, E.CH, &E.st->status);
-  if (__any_sync(0xffffffffu, mv)) {
-    const bool cv = mv && mark_bit(E.p.bmB, v);
-    warp_push(nq, nc, E.g.len, cv ? v : -1, true, E.CH, &E.st->status);
-  }
+__device__ __forceinline__ void push_marked(Env& E, const QueueBufs& nq, QCount* nc, int u, bool want) {
+  const bool claim = want && mark_bit(E.p.bmB, u);
+  if (__any_sync(0xffffffffu, claim))
+    warp_push(nq, nc, E.g.len, claim ? u : -1, true, M_MEX_ALL, E.CH, &E.st->status);
 }
 
 __device__ void expand_unit(Env& E, int4 un, const QueueBufs& nq, QCount* nc) {
@@ -344,18 +393,33 @@ __device__ void expand_unit(Env& E, int4 un, const QueueBufs& nq, QCount* nc) {
   R.v = v;
   R.cv = g.color[v];
   R.pv = E.variant == DC_HI ? g.prev[v] : g.prop[v];
-  for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
-    const int s = s0 + lane_id();
-    bool mu = false, mv = false;
-    int u = -1;
-    if (s < s_hi) {
-      u = g.adj[o + s];
-      if (u >= 0) {
-        ++E.my_scanned;
-        eligible(E, R, u, &mu, &mv);
-      }
+  for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
+    const int base = r0 + lane_id() * 4;
+    int4 q = make_int4(-1, -1, -1, -1);
+    if (base < s_hi) q = __ldg(reinterpret_cast<const int4*>(g.adj + o + base));
+    const int uu[4] = {q.x, q.y, q.z, q.w};
+    bool ok[4], mu[4], mv[4];
+    int cc[4], pp[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ok[j] = base + j < s_hi && uu[j] >= 0;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? g.color[uu[j]] : 0;
+    if (E.variant != DC_HI) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) pp[j] = ok[j] ? g.prop[uu[j]] : 0;
     }
-    mark_and_push(E, nq, nc, u, mu, v, mv);
+    bool anyv = false;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      mu[j] = mv[j] = false;
+      if (!ok[j]) continue;
+      ++E.my_scanned;
+      eligible(E, R, uu[j], cc[j], pp[j], &mu[j], &mv[j]);
+      anyv |= mv[j];
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) push_marked(E, nq, nc, uu[j], mu[j]);
+    push_marked(E, nq, nc, v, anyv);
   }
 }
 
@@ -372,25 +436,36 @@ __device__ void expand_batchA(Env& E, const QueueBufs& fq, long long cA, long lo
   const int incl = warp_incl_scan(L);
   const int T = __shfl_sync(0xffffffffu, incl, 31);
   const int excl = incl - L;
-  for (int s0 = 0; s0 < T; s0 += 32) {
-    const int s = s0 + lane_id();
-    const int j = find_owner(excl, s);
-    Rule R;
-    R.v = __shfl_sync(0xffffffffu, v, j);
-    R.cv = __shfl_sync(0xffffffffu, cv, j);
-    R.pv = __shfl_sync(0xffffffffu, pv, j);
-    const long long oj = __shfl_sync(0xffffffffu, o, j);
-    const int ej = __shfl_sync(0xffffffffu, excl, j);
-    bool mu = false, mv = false;
-    int u = -1;
-    if (s < T) {
-      u = g.adj[oj + (s - ej)];
-      if (u >= 0) {
-        ++E.my_scanned;
-        eligible(E, R, u, &mu, &mv);
-      }
+  for (int s0 = 0; s0 < T; s0 += 128) {
+    Rule R[4];
+    int uu[4], cc[4], pp[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int s = s0 + r * 32 + lane_id();
+      const int j = find_owner(excl, s);
+      R[r].v = __shfl_sync(0xffffffffu, v, j);
+      R[r].cv = __shfl_sync(0xffffffffu, cv, j);
+      R[r].pv = __shfl_sync(0xffffffffu, pv, j);
+      const long long oj = __shfl_sync(0xffffffffu, o, j);
+      const int ej = __shfl_sync(0xffffffffu, excl, j);
+      uu[r] = s < T ? g.adj[oj + (s - ej)] : -1;
     }
-    mark_and_push(E, nq, nc, u, mu, R.v, mv);
+#pragma unroll
+    for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? g.color[uu[r]] : 0;
+    if (E.variant != DC_HI) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) pp[r] = uu[r] >= 0 ? g.prop[uu[r]] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      bool mu = false, mv = false;
+      if (uu[r] >= 0) {
+        ++E.my_scanned;
+        eligible(E, R[r], uu[r], cc[r], pp[r], &mu, &mv);
+      }
+      push_marked(E, nq, nc, uu[r], mu);
+      push_marked(E, nq, nc, R[r].v, mv);
+    }
   }
 }
 
@@ -490,7 +565,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
     }
     if (f0) {
       const bool claim = push >= 0 && mark_bit(E.p.bmB, push);
-      warp_push(*f0, f0c, g.len, claim ? push : -1, true, E.CH, &E.st->status);
+      warp_push(*f0, f0c, g.len, claim ? push : -1, true, M_MEX_ALL, E.CH, &E.st->status);
     }
   }
   const int m = __reduce_max_sync(0xffffffffu, cmax_local);
@@ -502,7 +577,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
 
 }  // namespace
 
-__global__ void __launch_bounds__(kThreads) recolor_kernel(RecolorParams p) {
+__global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   __shared__ Shared sh;
   Env E;
   E.p.bmA = p.bmA;
@@ -548,7 +623,7 @@ __global__ void __launch_bounds__(kThreads) recolor_kernel(RecolorParams p) {
         p.lflag[i] = (c.inst == 1 && g.color[c.node1] == g.color[c.node2]) ? 1 : 0;
       }
       const bool claim = t >= 0 && mark_bit(p.bmA, t);
-      warp_push(B2, &st->q[Q_S1], g.len, claim ? t : -1, true, E.CH, &st->status);
+      warp_push(B2, &st->q[Q_S1], g.len, claim ? t : -1, true, M_MEX_ALL, E.CH, &st->status);
     }
     if (!grid_sync(st, bar)) return;
     // D2
@@ -572,9 +647,9 @@ __global__ void __launch_bounds__(kThreads) recolor_kernel(RecolorParams p) {
         }
       }
       const bool ca = a >= 0 && mark_bit(p.bmA, a);
-      warp_push(B2, &st->q[Q_S2E], g.len, ca ? a : -1, false, E.CH, &st->status);
+      warp_push(B2, &st->q[Q_S2E], g.len, ca ? a : -1, false, M_DISTINCT, E.CH, &st->status);
       const bool cb = b >= 0 && mark_bit(p.bmA, b);
-      warp_push(B2, &st->q[Q_S2E], g.len, cb ? b : -1, false, E.CH, &st->status);
+      warp_push(B2, &st->q[Q_S2E], g.len, cb ? b : -1, false, M_DISTINCT, E.CH, &st->status);
     }
     if (!grid_sync(st, bar)) return;
     // I2: saturation sizes
@@ -590,7 +665,7 @@ __global__ void __launch_bounds__(kThreads) recolor_kernel(RecolorParams p) {
         t = ld_cg(&p.sat[c.node1]) < ld_cg(&p.sat[c.node2]) ? c.node1 : c.node2;
       }
       const bool claim = t >= 0 && mark_bit(p.bmC, t);
-      warp_push(B1, &st->q[Q_S2T], g.len, claim ? t : -1, true, E.CH, &st->status);
+      warp_push(B1, &st->q[Q_S2T], g.len, claim ? t : -1, true, M_MEX_ALL, E.CH, &st->status);
     }
     phase_commit(E, B2, &st->q[Q_S2E], C_CLEAR_A, nullptr, nullptr, gwarp, nwarps, nullptr,
                  nullptr);
@@ -616,9 +691,9 @@ __global__ void __launch_bounds__(kThreads) recolor_kernel(RecolorParams p) {
         }
       }
       const bool ca = a >= 0 && mark_bit(p.bmA, a);
-      warp_push(B2, &st->q[Q_S1], g.len, ca ? a : -1, true, E.CH, &st->status);
+      warp_push(B2, &st->q[Q_S1], g.len, ca ? a : -1, true, M_MEX_ALL, E.CH, &st->status);
       const bool cb = b >= 0 && mark_bit(p.bmA, b);
-      warp_push(B2, &st->q[Q_S1], g.len, cb ? b : -1, true, E.CH, &st->status);
+      warp_push(B2, &st->q[Q_S1], g.len, cb ? b : -1, true, M_MEX_ALL, E.CH, &st->status);
     }
     if (!grid_sync(st, bar)) return;
     // H2
