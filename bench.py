@@ -428,6 +428,8 @@ def run_ours(args, dist: Dist):
             "iterations_per_batch": [int(s.iterations) for s in stats],
             "struct_ms_per_batch": str_ms / K,
             "recolor_ms_per_batch": rec_ms / K,
+            "phase_ms_per_batch": {k: round(sum(s.phase_ms[i] for s in stats) / K, 3)
+                                   for i, k in enumerate(("seeding", "find_eligible", "mex", "commit"))},
             "slots_scanned_per_batch": scanned / K,
             "max_color": int(max(s.max_color for s in stats)),
             "conflicts_after": int(conflicts),

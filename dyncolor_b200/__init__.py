@@ -66,10 +66,13 @@ class Stats(C.Structure):
         ("device_ms", C.c_double),
         ("struct_ms", C.c_double),
         ("recolor_ms", C.c_double),
+        ("phase_ms", C.c_double * 6),
     ]
 
     def as_dict(self):
-        return {f: getattr(self, f) for f, _ in self._fields_}
+        d = {f: getattr(self, f) for f, _ in self._fields_}
+        d["phase_ms"] = list(self.phase_ms)
+        return d
 
 
 class GraphInfo(C.Structure):

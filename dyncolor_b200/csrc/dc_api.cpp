@@ -451,6 +451,7 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
     out->device_ms = ms;
     out->struct_ms = ms_s;
     out->recolor_ms = ms_r;
+    for (int i = 0; i < 6; ++i) out->phase_ms[i] = (double)h.phase_ns[i] * 1e-6;
   }
   return rc;
 }

@@ -71,6 +71,7 @@ struct DevState {
   unsigned long long edges_inserted;  // directed entries (2 per undirected edge)
   unsigned long long edges_deleted;
   unsigned long long rows_relocated;
+  unsigned long long phase_ns[6];     // recolour launch: seeding, find-eligible, mex, commit, 2 spare
 };
 
 struct GraphDev {

@@ -38,6 +38,7 @@ enum Mode { M_MEX_ALL = 0, M_MEX_PRIOR = 1, M_DISTINCT = 2 };
 
 struct Shared {
   unsigned mask[kWarps][kMaskWords];  // per-warp colour window
+  int pbuf[kWarps][64];               // per-warp buffer of newly marked vertices
   long long swll[kWarps];
 };
 
@@ -224,18 +225,21 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
   __syncwarp();
   const int pv = mode == M_MEX_PRIOR ? g.prop[v] : 0;
   unsigned long long lm = 0;  // colours < 64 seen by this lane
-  // Four slots per lane per round: one aligned 16-byte load (rows start on
-  // 4-slot boundaries and hold capacity up to a multiple of 4) and four
-  // independent colour gathers in flight.
+  // Four slots per lane per round, lane l taking slots r0 + l + 32 j: every
+  // load is coalesced across the warp, and because rows are kept sorted by
+  // neighbour id, the colour gathers of one instruction fall on nearby
+  // addresses in dense rows.  Four independent gathers are in flight.
   for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
-    const int base = r0 + lane_id() * 4;
-    int4 q = make_int4(-1, -1, -1, -1);
-    if (base < s_hi) q = __ldg(reinterpret_cast<const int4*>(g.adj + o + base));
-    const int uu[4] = {q.x, q.y, q.z, q.w};
+    int uu[4];
     bool ok[4];
     int cc[4], pp[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) ok[j] = base + j < s_hi && uu[j] >= 0;
+    for (int j = 0; j < 4; ++j) {
+      const int sidx = r0 + j * 32 + lane_id();
+      uu[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) ok[j] = uu[j] >= 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? g.color[uu[j]] : 0;
     if (mode == M_MEX_PRIOR) {
@@ -376,14 +380,46 @@ __device__ __forceinline__ void eligible(const Env& E, const Rule& R, int u, int
   }
 }
 
-__device__ __forceinline__ void push_marked(Env& E, const QueueBufs& nq, QCount* nc, int u, bool want) {
-  const bool claim = want && mark_bit(E.p.bmB, u);
-  if (__any_sync(0xffffffffu, claim))
-    warp_push(nq, nc, E.g.len, claim ? u : -1, true, M_MEX_ALL, E.CH, &E.st->status);
+// Newly marked vertices collect in a per-warp shared buffer and are pushed
+// into the next queue 32 at a time, so every push round (row length gather,
+// class split, queue counters) runs with a full warp.
+struct PushBuf {
+  int* buf;  // sh.pbuf[warp]
+  int cnt;   // warp-uniform
+};
+
+__device__ __forceinline__ void flush(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int k) {
+  const int u = lane_id() < k ? pb.buf[lane_id()] : -1;
+  __syncwarp();
+  warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CH, &E.st->status);
+  // keep the remainder at the front
+  const int rest = pb.cnt - k;
+  if (lane_id() < rest) pb.buf[lane_id()] = pb.buf[k + lane_id()];  // rest <= 31 < k
+  __syncwarp();
+  pb.cnt = rest;
 }
 
-__device__ void expand_unit(Env& E, int4 un, const QueueBufs& nq, QCount* nc) {
+// Claims u (bit not yet set: the preloaded word says so and the atomic
+// confirms) and appends the claimed vertices to the warp buffer.  All lanes
+// must call.
+__device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int u,
+                                      bool want, unsigned word) {
+  bool got = false;
+  if (want) {
+    const unsigned bit = 1u << (u & 31);
+    if (!(word & bit)) got = !(atomicOr(E.p.bmB + (u >> 5), bit) & bit);
+  }
+  const unsigned bal = __ballot_sync(0xffffffffu, got);
+  if (!bal) return;
+  if (got) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = u;
+  __syncwarp();
+  pb.cnt += __popc(bal);
+  if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
+}
+
+__device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
+  const unsigned* bm = E.p.bmB;
   const int v = un.x;
   const int L = g.len[v];
   const long long o = g.off[v];
@@ -393,39 +429,46 @@ __device__ void expand_unit(Env& E, int4 un, const QueueBufs& nq, QCount* nc) {
   R.v = v;
   R.cv = g.color[v];
   R.pv = E.variant == DC_HI ? g.prev[v] : g.prop[v];
+  bool markv = false;
   for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
-    const int base = r0 + lane_id() * 4;
-    int4 q = make_int4(-1, -1, -1, -1);
-    if (base < s_hi) q = __ldg(reinterpret_cast<const int4*>(g.adj + o + base));
-    const int uu[4] = {q.x, q.y, q.z, q.w};
-    bool ok[4], mu[4], mv[4];
-    int cc[4], pp[4];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) ok[j] = base + j < s_hi && uu[j] >= 0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? g.color[uu[j]] : 0;
-    if (E.variant != DC_HI) {
-#pragma unroll
-      for (int j = 0; j < 4; ++j) pp[j] = ok[j] ? g.prop[uu[j]] : 0;
-    }
-    bool anyv = false;
+    int uu[4], cc[4], pp[4];
+    unsigned ww[4];
+    bool mu[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      mu[j] = mv[j] = false;
-      if (!ok[j]) continue;
-      ++E.my_scanned;
-      eligible(E, R, uu[j], cc[j], pp[j], &mu[j], &mv[j]);
-      anyv |= mv[j];
+      const int sidx = r0 + j * 32 + lane_id();
+      uu[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
+    }
+    // colour (and priority) gathers and bitmap words depend only on u
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      cc[j] = uu[j] >= 0 ? g.color[uu[j]] : 0;
+      ww[j] = uu[j] >= 0 ? ld_cg(bm + (uu[j] >> 5)) : ~0u;
+    }
+    if (E.variant != DC_HI) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) pp[j] = uu[j] >= 0 ? g.prop[uu[j]] : 0;
     }
 #pragma unroll
-    for (int j = 0; j < 4; ++j) push_marked(E, nq, nc, uu[j], mu[j]);
-    push_marked(E, nq, nc, v, anyv);
+    for (int j = 0; j < 4; ++j) {
+      mu[j] = false;
+      if (uu[j] < 0) continue;
+      ++E.my_scanned;
+      bool mv;
+      eligible(E, R, uu[j], cc[j], pp[j], &mu[j], &mv);
+      markv |= mv;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
   }
+  const bool mv = __any_sync(0xffffffffu, markv);
+  claim(E, pb, nq, nc, v, mv && lane_id() == 0, mv ? ld_cg(bm + (v >> 5)) : ~0u);
 }
 
-__device__ void expand_batchA(Env& E, const QueueBufs& fq, long long cA, long long b,
+__device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long long cA, long long b,
                               const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
+  const unsigned* bm = E.p.bmB;
   const long long idx = b * 32 + lane_id();
   const bool valid = idx < cA;
   const int v = valid ? fq.itemsA[idx] : 0;
@@ -439,6 +482,7 @@ __device__ void expand_batchA(Env& E, const QueueBufs& fq, long long cA, long lo
   for (int s0 = 0; s0 < T; s0 += 128) {
     Rule R[4];
     int uu[4], cc[4], pp[4];
+    unsigned ww[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       const int s = s0 + r * 32 + lane_id();
@@ -451,7 +495,10 @@ __device__ void expand_batchA(Env& E, const QueueBufs& fq, long long cA, long lo
       uu[r] = s < T ? g.adj[oj + (s - ej)] : -1;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? g.color[uu[r]] : 0;
+    for (int r = 0; r < 4; ++r) {
+      cc[r] = uu[r] >= 0 ? g.color[uu[r]] : 0;
+      ww[r] = uu[r] >= 0 ? ld_cg(bm + (uu[r] >> 5)) : ~0u;
+    }
     if (E.variant != DC_HI) {
 #pragma unroll
       for (int r = 0; r < 4; ++r) pp[r] = uu[r] >= 0 ? g.prop[uu[r]] : 0;
@@ -463,26 +510,30 @@ __device__ void expand_batchA(Env& E, const QueueBufs& fq, long long cA, long lo
         ++E.my_scanned;
         eligible(E, R[r], uu[r], cc[r], pp[r], &mu, &mv);
       }
-      push_marked(E, nq, nc, uu[r], mu);
-      push_marked(E, nq, nc, R[r].v, mv);
+      claim(E, pb, nq, nc, uu[r], mu, ww[r]);
+      claim(E, pb, nq, nc, R[r].v, mv, mv ? ld_cg(bm + (R[r].v >> 5)) : ~0u);
     }
   }
 }
 
-__device__ void phase_expand(Env& E, const QueueBufs& fq, const QCount* fc, const QueueBufs& nq,
-                             QCount* nc, unsigned long long* ctr) {
+__device__ void phase_expand(Env& E, Shared& sh, const QueueBufs& fq, const QCount* fc,
+                             const QueueBufs& nq, QCount* nc, unsigned long long* ctr) {
   const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
   const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
   const long long nAb = (cA + 31) / 32;
   const long long total = cU + nAb;
+  PushBuf pb;
+  pb.buf = sh.pbuf[warp_id()];
+  pb.cnt = 0;
   while (true) {
     const long long i = grab(ctr);
     if (i >= total) break;
     if (i < cU)
-      expand_unit(E, fq.units[i], nq, nc);
+      expand_unit(E, pb, fq.units[i], nq, nc);
     else
-      expand_batchA(E, fq, cA, i - cU, nq, nc);
+      expand_batchA(E, pb, fq, cA, i - cU, nq, nc);
   }
+  if (pb.cnt > 0) flush(E, pb, nq, nc, pb.cnt);
 }
 
 // ---------------------------------------------------------------------
@@ -601,6 +652,17 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     if (leader) st->wctr[(ps + 1) % 3] = 0ull;  // next phase's counter (last used 2 phases ago)
     return &st->wctr[ps % 3];
   };
+  // Phase timer: CTA 0 thread 0 reads %globaltimer after each barrier and
+  // charges the elapsed time to the phase kind that just ended.
+  unsigned long long t_last = leader ? globaltimer_ns() : 0ull;
+  unsigned long long acc[6] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+  auto lap = [&](int kind) {
+    if (leader) {
+      const unsigned long long t = globaltimer_ns();
+      acc[kind] += t - t_last;
+      t_last = t;
+    }
+  };
   const QueueBufs& B0 = p.qb[0];  // F0 and even loop queues
   const QueueBufs& B1 = p.qb[1];  // odd loop queues, HI insertion targets
   const QueueBufs& B2 = p.qb[2];  // seeding sets
@@ -709,6 +771,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   phase_commit(E, B0, &st->q[Q_LOOP0], C_CLEAR_B, nullptr, nullptr, gwarp, nwarps, nullptr,
                nullptr);
   if (!grid_sync(st, bar)) return;
+  lap(0);
 
   // ======================= loop =======================
   {
@@ -733,9 +796,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         z->countU = 0;
         z->masks = 0;
       }
-      phase_expand(E, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
+      phase_expand(E, sh, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
       ++ps;
       if (!grid_sync(st, bar)) return;
+      lap(1);
       const QCount* nc = &st->q[ns];
       const long long nq = (long long)(ld_cg(&nc->countA) + ld_cg(&nc->countU));
       if (p.variant == DC_HI && nq == 0) break;
@@ -744,15 +808,20 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
       ++ps;
       if (!grid_sync(st, bar)) return;
+      lap(2);
       // C
       phase_commit(E, p.qb[nb], nc, C_LOOP, nullptr, nullptr, gwarp, nwarps, &st->frontier_total,
                    &st->chg[it & 1]);
       if (!grid_sync(st, bar)) return;
+      lap(3);
       if (p.variant == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;
       fs = ns;
       fb = nb;
     }
-    if (leader) st->iterations = (unsigned long long)it;
+    if (leader) {
+      st->iterations = (unsigned long long)it;
+      for (int i = 0; i < 6; ++i) st->phase_ns[i] = acc[i];
+    }
   }
   const long long sc = warp_sum_ll(E.my_scanned);
   if (lane_id() == 0 && sc) atomicAdd(&st->slots_scanned, (unsigned long long)sc);

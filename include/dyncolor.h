@@ -91,6 +91,8 @@ typedef struct {
   double device_ms;       /* device time of the batch (CUDA events) */
   double struct_ms;       /* of which the structural-update launch */
   double recolor_ms;      /* of which the seeding + recolour launch */
+  double phase_ms[6];     /* recolour launch split: seeding, find-eligible, mex, commit,
+                             2 reserved */
 } dc_stats;
 
 typedef struct {

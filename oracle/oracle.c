@@ -146,6 +146,8 @@ static int32_t max_len(const orc_graph* g) {
 
 static int g_threads = 0;
 void orc_set_threads(int nthreads) { g_threads = nthreads; }
+static int g_instrument = 0;
+void orc_set_instrument(int on) { g_instrument = on; }
 
 static int nthreads_now(void) {
 #ifdef _OPENMP
@@ -675,6 +677,19 @@ int orc_apply_batch(orc_graph* g, int variant, int schedule, const orc_change* c
       compact(&R);
       memset(R.mark, 0, nn);
       S.frontier_total += R.count;
+      if (g_instrument) {
+        /* edges with both ends in this frontier (R.list), via a membership array */
+        uint8_t* inq = (uint8_t*)calloc(nn, 1);
+        for (int64_t i = 0; i < R.count; ++i) inq[R.list[i]] = 1;
+        for (int64_t i = 0; i < R.count; ++i) {
+          int32_t t = R.list[i];
+          for (int32_t j = 0; j < g->len[t]; ++j) {
+            int32_t u = g->row[t][j];
+            if (u >= 0 && inq[u]) S.internal_pairs++;
+          }
+        }
+        free(inq);
+      }
       /* recolorNeighbor: HI/gpuFunctions_undir.cuh:264-284 (always sets
        * change), HB/gpuFunctions_undir.cuh:295-314 (only on a change). */
       if (schedule == ORC_SNAPSHOT) {

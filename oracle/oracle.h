@@ -67,6 +67,9 @@ typedef struct {
   int64_t changed_vertices;/* vertices whose final color differs from the start */
   int32_t status;          /* ORC_OK or ORC_E_ITER_LIMIT */
   int32_t max_color;       /* max color after the batch */
+  int64_t internal_pairs;  /* instrumentation: sum over iterations of live
+                              directed edges with both ends in the recolor
+                              frontier (only with orc_set_instrument(1)) */
 } orc_stats;
 
 typedef struct orc_graph orc_graph;
@@ -96,6 +99,7 @@ int orc_is_greedy_id_order(const orc_graph* g);
 int orc_greedy_id_order(orc_graph* g);
 int32_t orc_num_vertices(const orc_graph* g);
 void orc_set_threads(int nthreads);
+void orc_set_instrument(int on);
 
 #ifdef __cplusplus
 }

@@ -36,6 +36,7 @@ class Stats(C.Structure):
         ("changed_vertices", C.c_int64),
         ("status", C.c_int32),
         ("max_color", C.c_int32),
+        ("internal_pairs", C.c_int64),
     ]
 
     def as_dict(self):
@@ -71,6 +72,7 @@ def lib():
         L.orc_is_greedy_id_order.argtypes = [P]
         L.orc_greedy_id_order.argtypes = [P]
         L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_set_instrument.argtypes = [C.c_int]
         _lib = L
     return _lib
 
