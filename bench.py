@@ -431,6 +431,8 @@ def run_ours(args, dist: Dist):
             "phase_ms_per_batch": {k: round(sum(s.phase_ms[i] for s in stats) / K, 3)
                                    for i, k in enumerate(("seeding", "find_eligible", "mex", "commit"))},
             "slots_scanned_per_batch": scanned / K,
+            "slots_read_per_batch": sum(s.slots_read for s in stats) / K,
+            "pairs_per_batch": sum(s.pairs for s in stats) / K,
             "max_color": int(max(s.max_color for s in stats)),
             "conflicts_after": int(conflicts),
             "workload_gen_s": round(w["gen_s"], 1),

@@ -67,6 +67,8 @@ class Stats(C.Structure):
         ("struct_ms", C.c_double),
         ("recolor_ms", C.c_double),
         ("phase_ms", C.c_double * 6),
+        ("slots_read", C.c_int64),
+        ("pairs", C.c_int64),
     ]
 
     def as_dict(self):

@@ -436,6 +436,7 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   if (rc != DC_OK && recolor) {
     dc_status s2 = reset_bitmaps(ctx);
     if (s2 != DC_OK) return s2;
+    DC_CK(launch_color_unmark(graph_dev(ctx), ctx->stream));
   }
   if (out) {
     std::memset(out, 0, sizeof(*out));
@@ -452,6 +453,8 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
     out->struct_ms = ms_s;
     out->recolor_ms = ms_r;
     for (int i = 0; i < 6; ++i) out->phase_ms[i] = (double)h.phase_ns[i] * 1e-6;
+    out->slots_read = (int64_t)h.slots_read;
+    out->pairs = 0;
   }
   return rc;
 }
@@ -640,7 +643,8 @@ dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   if (n != ctx->n || (n > 0 && !colors)) return fail(ctx, DC_E_INVAL, "colour array size differs from n");
   for (int32_t v = 0; v < n; ++v)
-    if (colors[v] < 0) return fail(ctx, DC_E_INVAL, "negative colour at vertex " + std::to_string(v));
+    if (colors[v] < 0 || colors[v] > kColorMask)
+      return fail(ctx, DC_E_INVAL, "colour outside [0, 2^30) at vertex " + std::to_string(v));
   cudaSetDevice(ctx->device);
   if (n > 0) DC_CK(cudaMemcpyAsync(ctx->color, colors, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
   DC_CK(launch_color_max(graph_dev(ctx), ctx->st, ctx->stream));

@@ -24,6 +24,10 @@ constexpr int kMaskWords = 128;     // colour window per warp: 4096 colours
 constexpr int kMaskBits = kMaskWords * 32;
 constexpr int kStructChunk = 1024;  // slots per unit in the structural row scans
 constexpr int kTomb = -1;           // tombstoned adjacency slot
+// During the recolour loop, bit 30 of color[v] marks v for the next
+// frontier; colours are below 2^30.  The commit's store clears it.
+constexpr unsigned kMarkBit = 1u << 30;
+constexpr int kColorMask = (1 << 30) - 1;
 constexpr int kNumQueues = 6;       // logical queue counter slots
 constexpr int kUnitSlotsDefault = 2048;  // adjacency slots per warp work unit
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
@@ -71,6 +75,7 @@ struct DevState {
   unsigned long long edges_inserted;  // directed entries (2 per undirected edge)
   unsigned long long edges_deleted;
   unsigned long long rows_relocated;
+  unsigned long long slots_read;      // adjacency entries the kernels actually read
   unsigned long long phase_ns[6];     // recolour launch: seeding, find-eligible, mex, commit, 2 spare
 };
 
@@ -154,6 +159,8 @@ int recolor_kernel_occupancy();
 cudaError_t launch_validate(const GraphDev& g, unsigned long long* out, cudaStream_t s);
 cudaError_t launch_color_max(const GraphDev& g, DevState* st, cudaStream_t s);
 cudaError_t launch_count_live(const GraphDev& g, unsigned long long* out, cudaStream_t s);
+// Clears loop marks left in the colour array by an aborted launch.
+cudaError_t launch_color_unmark(const GraphDev& g, cudaStream_t s);
 // Repacks rows of g into new arrays (off2/cap2/adj2) with the given slack.
 cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* adj2,
                           long long cap_slots, float slack, unsigned long long* used,

@@ -44,6 +44,12 @@ __global__ void count_live_kernel(GraphDev g, unsigned long long* out) {
   if (lane_id() == 0 && s) atomicAdd(out, (unsigned long long)s);
 }
 
+__global__ void color_unmark_kernel(GraphDev g) {
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < g.n;
+       v += (long long)gridDim.x * blockDim.x)
+    g.color[v] &= kColorMask;
+}
+
 __device__ __forceinline__ long long packed_cap(int live, float slack) {
   if (live <= 0) return 0;
   long long want = (long long)ceilf((float)live * slack);
@@ -168,6 +174,11 @@ cudaError_t launch_count_live(const GraphDev& g, unsigned long long* out, cudaSt
   cudaError_t e = cudaMemsetAsync(out, 0, sizeof(unsigned long long), s);
   if (e != cudaSuccess) return e;
   count_live_kernel<<<misc_grid(g.n, kMiscThreads), kMiscThreads, 0, s>>>(g, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_color_unmark(const GraphDev& g, cudaStream_t s) {
+  color_unmark_kernel<<<misc_grid(g.n, kMiscThreads), kMiscThreads, 0, s>>>(g);
   return cudaGetLastError();
 }
 

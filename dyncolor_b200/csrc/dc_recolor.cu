@@ -156,7 +156,7 @@ __device__ int slow_mex(Env& E, unsigned* sm, int v, int mode) {
       if (s < L) {
         const int u = g.adj[o + s];
         if (u >= 0 && (mode != M_MEX_PRIOR || is_prior(g.prop[u], u, pv, v))) {
-          const int c = g.color[u] - w0;
+          const int c = (g.color[u] & kColorMask) - w0;
           if (c >= 0 && c < kMaskBits) atomicOr(&sm[c >> 5], 1u << (c & 31));
         }
       }
@@ -182,7 +182,7 @@ __device__ int slow_distinct(Env& E, unsigned* sm, int v, int cmax) {
       if (s < L) {
         const int u = g.adj[o + s];
         if (u >= 0) {
-          const int c = g.color[u] - w0;
+          const int c = (g.color[u] & kColorMask) - w0;
           if (c >= 0 && c < kMaskBits) atomicOr(&sm[c >> 5], 1u << (c & 31));
         }
       }
@@ -241,7 +241,7 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
 #pragma unroll
     for (int j = 0; j < 4; ++j) ok[j] = uu[j] >= 0;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? g.color[uu[j]] : 0;
+    for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? (g.color[uu[j]] & kColorMask) : 0;
     if (mode == M_MEX_PRIOR) {
 #pragma unroll
       for (int j = 0; j < 4; ++j) pp[j] = ok[j] ? g.prop[uu[j]] : 0;
@@ -323,7 +323,7 @@ __device__ void reduce_batchA(Env& E, Shared& sh, const QueueBufs& qb, long long
       uu[r] = s < T ? g.adj[oj + (s - ej)] : -1;
     }
 #pragma unroll
-    for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? g.color[uu[r]] : 0;
+    for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? (g.color[uu[r]] & kColorMask) : 0;
     if (mode == M_MEX_PRIOR) {
 #pragma unroll
       for (int r = 0; r < 4; ++r) pp[r] = uu[r] >= 0 ? g.prop[uu[r]] : 0;
@@ -399,16 +399,15 @@ __device__ __forceinline__ void flush(Env& E, PushBuf& pb, const QueueBufs& nq, 
   pb.cnt = rest;
 }
 
-// Claims u (bit not yet set: the preloaded word says so and the atomic
-// confirms) and appends the claimed vertices to the warp buffer.  All lanes
-// must call.
+// Claims u for the next frontier: sets the mark bit of its colour word
+// unless the preloaded word already has it (the atomic decides races), and
+// appends the vertices this warp marked first to the warp buffer.  All
+// lanes must call.
 __device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int u,
                                       bool want, unsigned word) {
   bool got = false;
-  if (want) {
-    const unsigned bit = 1u << (u & 31);
-    if (!(word & bit)) got = !(atomicOr(E.p.bmB + (u >> 5), bit) & bit);
-  }
+  if (want && !(word & kMarkBit))
+    got = !(atomicOr(reinterpret_cast<unsigned*>(E.g.color + u), kMarkBit) & kMarkBit);
   const unsigned bal = __ballot_sync(0xffffffffu, got);
   if (!bal) return;
   if (got) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = u;
@@ -419,7 +418,6 @@ __device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, 
 
 __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
-  const unsigned* bm = E.p.bmB;
   const int v = un.x;
   const int L = g.len[v];
   const long long o = g.off[v];
@@ -427,7 +425,7 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
   const int s_hi = min(L, s_lo + E.CH);
   Rule R;
   R.v = v;
-  R.cv = g.color[v];
+  R.cv = g.color[v] & kColorMask;
   R.pv = E.variant == DC_HI ? g.prev[v] : g.prop[v];
   bool markv = false;
   for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
@@ -439,11 +437,11 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
       const int sidx = r0 + j * 32 + lane_id();
       uu[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
     }
-    // colour (and priority) gathers and bitmap words depend only on u
+    // one gather gives u's colour and its next-frontier mark
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      cc[j] = uu[j] >= 0 ? g.color[uu[j]] : 0;
-      ww[j] = uu[j] >= 0 ? ld_cg(bm + (uu[j] >> 5)) : ~0u;
+      ww[j] = uu[j] >= 0 ? (unsigned)g.color[uu[j]] : kMarkBit;
+      cc[j] = (int)(ww[j] & (unsigned)kColorMask);
     }
     if (E.variant != DC_HI) {
 #pragma unroll
@@ -462,19 +460,18 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
     for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
   }
   const bool mv = __any_sync(0xffffffffu, markv);
-  claim(E, pb, nq, nc, v, mv && lane_id() == 0, mv ? ld_cg(bm + (v >> 5)) : ~0u);
+  claim(E, pb, nq, nc, v, mv && lane_id() == 0, mv ? (unsigned)ld_cg(g.color + v) : kMarkBit);
 }
 
 __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long long cA, long long b,
                               const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
-  const unsigned* bm = E.p.bmB;
   const long long idx = b * 32 + lane_id();
   const bool valid = idx < cA;
   const int v = valid ? fq.itemsA[idx] : 0;
   const int L = valid ? g.len[v] : 0;
   const long long o = valid ? g.off[v] : 0;
-  const int cv = valid ? g.color[v] : 0;
+  const int cv = valid ? (g.color[v] & kColorMask) : 0;
   const int pv = valid ? (E.variant == DC_HI ? g.prev[v] : g.prop[v]) : 0;
   const int incl = warp_incl_scan(L);
   const int T = __shfl_sync(0xffffffffu, incl, 31);
@@ -496,8 +493,8 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      cc[r] = uu[r] >= 0 ? g.color[uu[r]] : 0;
-      ww[r] = uu[r] >= 0 ? ld_cg(bm + (uu[r] >> 5)) : ~0u;
+      ww[r] = uu[r] >= 0 ? (unsigned)g.color[uu[r]] : kMarkBit;
+      cc[r] = (int)(ww[r] & (unsigned)kColorMask);
     }
     if (E.variant != DC_HI) {
 #pragma unroll
@@ -511,7 +508,7 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
         eligible(E, R[r], uu[r], cc[r], pp[r], &mu, &mv);
       }
       claim(E, pb, nq, nc, uu[r], mu, ww[r]);
-      claim(E, pb, nq, nc, R[r].v, mv, mv ? ld_cg(bm + (R[r].v >> 5)) : ~0u);
+      claim(E, pb, nq, nc, R[r].v, mv, mv ? (unsigned)ld_cg(g.color + R[r].v) : kMarkBit);
     }
   }
 }
@@ -540,7 +537,7 @@ __device__ void phase_expand(Env& E, Shared& sh, const QueueBufs& fq, const QCou
 // COMMIT and line phases
 // ---------------------------------------------------------------------
 enum Commit {
-  C_LOOP = 0,     // prev (HI) and colour from ncolor, clear bmB
+  C_LOOP = 0,     // prev (HI) and colour from ncolor (clears the frontier mark)
   C_SEED_DEL = 1, // HI deleteEdge: commit if changed, F0 += v, clear bmA
   C_SEED_INS = 2, // HI insEdge: commit always, F0 += v, clear bmC
   C_SEED_HB = 3,  // HB processChangeEdge: commit if changed, F0 += v, clear bmA
@@ -576,12 +573,11 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
       switch (kind) {
         case C_LOOP: {
           const int nc = ld_cg(&E.p.ncolor[v]);
-          const int oc = g.color[v];
+          const int oc = ld_cg(g.color + v) & kColorMask;
           if (E.variant == DC_HI) g.prev[v] = oc;
           if (nc != oc) changed = true;
-          g.color[v] = nc;
+          g.color[v] = nc;  // also clears the frontier mark
           cmax_local = max(cmax_local, nc);
-          E.p.bmB[v >> 5] = 0u;
           break;
         }
         case C_SEED_DEL:
@@ -824,7 +820,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     }
   }
   const long long sc = warp_sum_ll(E.my_scanned);
-  if (lane_id() == 0 && sc) atomicAdd(&st->slots_scanned, (unsigned long long)sc);
+  if (lane_id() == 0 && sc) {
+    atomicAdd(&st->slots_scanned, (unsigned long long)sc);
+    atomicAdd(&st->slots_read, (unsigned long long)sc);  // every scan reads its row once
+  }
 }
 
 cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s) {

@@ -93,6 +93,9 @@ typedef struct {
   double recolor_ms;      /* of which the seeding + recolour launch */
   double phase_ms[6];     /* recolour launch split: seeding, find-eligible, mex, commit,
                              2 reserved */
+  int64_t slots_read;     /* adjacency entries the kernels actually read (the loop
+                             reads each frontier row once per iteration) */
+  int64_t pairs;          /* frontier-internal edges the fused loop deferred */
 } dc_stats;
 
 typedef struct {
@@ -121,7 +124,7 @@ void dc_destroy(dc_ctx* ctx);
 dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const int32_t* b,
                               int64_t m);
 
-/* initial-color (read_Input_Color): colours must be >= 0. */
+/* initial-color (read_Input_Color): colours must lie in [0, 2^30). */
 dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n);
 
 /* apply-update-batch from host memory (any host pointer; pinned is fastest).

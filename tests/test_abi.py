@@ -38,7 +38,7 @@ def test_options_default_and_status_strings():
     assert dc.lib().dc_options_default(ctypes.byref(opt)) == dc.OK
     assert opt.variant == dc.HI and opt.iter_cap > 0 and opt.slack > 1 and opt.unit_slots % 128 == 0
     assert dc.status_str(dc.E_ITER_LIMIT) == "iteration cap reached"
-    assert ctypes.sizeof(dc.Stats) == 136 and dc.CHANGE_DTYPE.itemsize == 12
+    assert ctypes.sizeof(dc.Stats) == 152 and dc.CHANGE_DTYPE.itemsize == 12
 
 
 def test_generators_deterministic_and_thread_independent():
