@@ -121,6 +121,8 @@ def lib() -> C.CDLL:
     L.dc_neighbors.argtypes = [P, C.c_int32, P, C.c_int32, C.POINTER(C.c_int32)]
     L.dc_graph_info_get.argtypes = [P, C.POINTER(GraphInfo)]
     L.dc_compact.argtypes = [P]
+    L.dc_partition_set.argtypes = [P, C.c_int32, P]
+    L.dc_graph_iterations.argtypes = [P, P, C.c_int32]
     L.dc_last_error.argtypes = [P]
     L.dc_last_error.restype = C.c_char_p
     L.dc_status_str.argtypes = [C.c_int]
@@ -280,6 +282,17 @@ class Context:
 
     def compact(self):
         self._check(lib().dc_compact(self._h), "dc_compact")
+
+    def set_partition(self, first):
+        """Batched mode: graph g owns vertices [first[g], first[g+1])."""
+        f = np.ascontiguousarray(first, dtype=np.int32)
+        self._check(lib().dc_partition_set(self._h, len(f) - 1, _ptr(f)), "dc_partition_set")
+        self.ngraphs = len(f) - 1
+
+    def graph_iterations(self) -> np.ndarray:
+        out = np.empty(self.ngraphs, dtype=np.int64)
+        self._check(lib().dc_graph_iterations(self._h, _ptr(out), self.ngraphs), "dc_graph_iterations")
+        return out
 
 
 # ---------------------------------------------------------------------------

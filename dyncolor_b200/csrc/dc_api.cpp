@@ -85,6 +85,15 @@ struct dc_ctx {
   unsigned* cta_cnt = nullptr;
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
+
+  // batched mode: disjoint union of ngraphs graphs
+  int ngraphs = 0;
+  int* first = nullptr;   // ngraphs + 1
+  int* gid = nullptr;     // n
+  int* gcnt = nullptr;    // 2 * ngraphs
+  int* gf0 = nullptr;     // ngraphs
+  int* giters = nullptr;  // ngraphs
+  int* gstate = nullptr;  // ngraphs
 };
 
 namespace {
@@ -301,6 +310,7 @@ StructParams struct_params(dc_ctx* ctx, const dc_change* ch, const int* la, cons
   p.relunits = ctx->relunits;
   p.cap_units = ctx->cap_units;
   p.cap_rel = ctx->cap_rel;
+  p.gid = ctx->ngraphs > 0 ? ctx->gid : nullptr;
   p.st = ctx->st;
   return p;
 }
@@ -320,6 +330,14 @@ RecolorParams recolor_params(dc_ctx* ctx, const dc_change* ch, long long k) {
   p.ncolor = ctx->ncolor;
   p.sat = ctx->sat;
   p.lflag = ctx->lflag;
+  if (ctx->ngraphs > 0) {
+    p.gid = ctx->gid;
+    p.ngraphs = ctx->ngraphs;
+    p.gcnt = ctx->gcnt;
+    p.gf0 = ctx->gf0;
+    p.giters = ctx->giters;
+    p.gstate = ctx->gstate;
+  }
   p.st = ctx->st;
   return p;
 }
@@ -397,6 +415,13 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
     DC_CK(launch_struct(struct_params(ctx, d_ch, la, lb, k), ctx->grid_struct, ctx->stream));
     DC_CK(cudaEventRecord(ctx->evm, ctx->stream));
     if (recolor) {
+      if (ctx->ngraphs > 0) {
+        const size_t G = (size_t)ctx->ngraphs;
+        DC_CK(cudaMemsetAsync(ctx->gcnt, 0, 2 * G * sizeof(int), ctx->stream));
+        DC_CK(cudaMemsetAsync(ctx->gf0, 0, G * sizeof(int), ctx->stream));
+        DC_CK(cudaMemsetAsync(ctx->giters, 0, G * sizeof(int), ctx->stream));
+        DC_CK(cudaMemsetAsync(ctx->gstate, 0, G * sizeof(int), ctx->stream));
+      }
       DC_CK(cudaMemcpyAsync(&ctx->st->pre_status, &ctx->st->status, sizeof(unsigned),
                             cudaMemcpyDeviceToDevice, ctx->stream));
       // fresh grid barrier and work counters for the second cooperative launch
@@ -572,6 +597,12 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->color);
   dfree(ctx, &ctx->prev);
   dfree(ctx, &ctx->prop);
+  dfree(ctx, &ctx->first);
+  dfree(ctx, &ctx->gid);
+  dfree(ctx, &ctx->gcnt);
+  dfree(ctx, &ctx->gf0);
+  dfree(ctx, &ctx->giters);
+  dfree(ctx, &ctx->gstate);
   dfree(ctx, &ctx->st);
   dfree(ctx, &ctx->d_scalar);
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
@@ -759,6 +790,48 @@ dc_status dc_compact(dc_ctx* ctx) {
   if (s != DC_OK) return s;
   if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
   DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+dc_status dc_partition_set(dc_ctx* ctx, int32_t ngraphs, const int32_t* first) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (ngraphs <= 0 || !first) return fail(ctx, DC_E_INVAL, "bad partition arguments");
+  if (first[0] != 0 || first[ngraphs] != ctx->n)
+    return fail(ctx, DC_E_INVAL, "partition must start at 0 and end at n");
+  for (int32_t g = 0; g < ngraphs; ++g)
+    if (first[g + 1] < first[g]) return fail(ctx, DC_E_INVAL, "partition offsets must not decrease");
+  cudaSetDevice(ctx->device);
+  const long long G = ngraphs;
+  dc_status s;
+  if ((s = dalloc(ctx, &ctx->first, G + 1, "partition offsets")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->gid, std::max(ctx->n, 1), "graph ids")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->gcnt, 2 * G, "graph counters")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->gf0, G, "graph counters")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->giters, G, "graph iterations")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &ctx->gstate, G, "graph states")) != DC_OK) return s;
+  DC_CK(cudaMemcpyAsync(ctx->first, first, (size_t)(G + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  DC_CK(cudaMemsetAsync(ctx->giters, 0, (size_t)G * sizeof(int), ctx->stream));
+  DC_CK(launch_partition(graph_dev(ctx), ctx->first, ngraphs, ctx->gid, ctx->d_scalar, ctx->stream));
+  DC_CK(cudaMemcpyAsync(ctx->h_scalar, ctx->d_scalar, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  if (ctx->h_scalar[0] != 0) {
+    ctx->ngraphs = 0;
+    return fail(ctx, DC_E_INVAL, std::to_string(ctx->h_scalar[0]) + " adjacency entries join two graphs");
+  }
+  ctx->ngraphs = ngraphs;
+  return DC_OK;
+}
+
+dc_status dc_graph_iterations(dc_ctx* ctx, int64_t* out, int32_t ngraphs) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (ctx->ngraphs == 0) return fail(ctx, DC_E_STATE, "no partition set");
+  if (ngraphs != ctx->ngraphs || !out) return fail(ctx, DC_E_INVAL, "output size differs from the partition");
+  cudaSetDevice(ctx->device);
+  std::vector<int> tmp((size_t)ngraphs);
+  DC_CK(cudaMemcpyAsync(tmp.data(), ctx->giters, (size_t)ngraphs * sizeof(int), cudaMemcpyDeviceToHost,
+                        ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  for (int32_t g = 0; g < ngraphs; ++g) out[g] = tmp[(size_t)g];
   return DC_OK;
 }
 

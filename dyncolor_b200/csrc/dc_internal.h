@@ -130,6 +130,7 @@ struct StructParams {
   int2* relunits;        // relocation copy units
   long long cap_units;
   long long cap_rel;
+  const int* gid;        // batched mode: vertex -> graph; lines must stay inside a graph
   DevState* st;
 };
 
@@ -147,6 +148,13 @@ struct RecolorParams {
   int* ncolor;           // n
   int* sat;              // n
   unsigned char* lflag;  // k
+  // Batched mode: the graph is a disjoint union of independent graphs.
+  const int* gid;        // vertex -> graph (nullptr: one graph)
+  int ngraphs;
+  int* gcnt;             // 2 * ngraphs: per-iteration activity of each graph (ring by parity)
+  int* gf0;              // ngraphs: vertices each graph put in frontier F0
+  int* giters;           // ngraphs: loop iterations of each graph
+  int* gstate;           // ngraphs: 0 not started, 1 running, 2 done
   DevState* st;
 };
 
@@ -161,6 +169,9 @@ cudaError_t launch_color_max(const GraphDev& g, DevState* st, cudaStream_t s);
 cudaError_t launch_count_live(const GraphDev& g, unsigned long long* out, cudaStream_t s);
 // Clears loop marks left in the colour array by an aborted launch.
 cudaError_t launch_color_unmark(const GraphDev& g, cudaStream_t s);
+// Batched mode: gid[v] from graph start offsets; counts edges crossing graphs.
+cudaError_t launch_partition(const GraphDev& g, const int* first, int ngraphs, int* gid,
+                             unsigned long long* cross, cudaStream_t s);
 // Repacks rows of g into new arrays (off2/cap2/adj2) with the given slack.
 cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* adj2,
                           long long cap_slots, float slack, unsigned long long* used,

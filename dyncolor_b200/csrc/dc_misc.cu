@@ -50,6 +50,37 @@ __global__ void color_unmark_kernel(GraphDev g) {
     g.color[v] &= kColorMask;
 }
 
+// gid[v] = graph of v (first[] ascending, first[0] = 0, first[ngraphs] = n),
+// then the number of live adjacency entries joining two graphs.
+__global__ void partition_gid_kernel(GraphDev g, const int* first, int ngraphs, int* gid) {
+  for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < g.n;
+       v += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = ngraphs;  // largest j with first[j] <= v
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (first[mid] <= v) lo = mid; else hi = mid;
+    }
+    gid[v] = lo;
+  }
+}
+
+__global__ void partition_cross_kernel(GraphDev g, const int* gid, unsigned long long* cross) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long bad = 0;
+  for (long long v = gw; v < g.n; v += nw) {
+    const long long o = g.off[v];
+    const int L = g.len[v];
+    const int gv = gid[v];
+    for (int s = lane_id(); s < L; s += 32) {
+      const int u = g.adj[o + s];
+      if (u >= 0 && gid[u] != gv) ++bad;
+    }
+  }
+  bad = warp_sum_ll(bad);
+  if (lane_id() == 0 && bad) atomicAdd(cross, (unsigned long long)bad);
+}
+
 __device__ __forceinline__ long long packed_cap(int live, float slack) {
   if (live <= 0) return 0;
   long long want = (long long)ceilf((float)live * slack);
@@ -179,6 +210,15 @@ cudaError_t launch_count_live(const GraphDev& g, unsigned long long* out, cudaSt
 
 cudaError_t launch_color_unmark(const GraphDev& g, cudaStream_t s) {
   color_unmark_kernel<<<misc_grid(g.n, kMiscThreads), kMiscThreads, 0, s>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_partition(const GraphDev& g, const int* first, int ngraphs, int* gid,
+                             unsigned long long* cross, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(cross, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  partition_gid_kernel<<<misc_grid(g.n, kMiscThreads), kMiscThreads, 0, s>>>(g, first, ngraphs, gid);
+  partition_cross_kernel<<<misc_grid((long long)g.n * 32, kMiscThreads), kMiscThreads, 0, s>>>(g, gid, cross);
   return cudaGetLastError();
 }
 

@@ -138,6 +138,12 @@ struct Env {
   int variant;
   int CH;
   long long my_scanned;
+  // batched mode (all nullptr for one graph)
+  const int* gid;
+  int* gpush;        // HI: pushes into the next frontier per graph, this iteration
+  int* gchg;         // HB: colour changes per graph, this iteration
+  const int* gskip;  // HB: graphs whose last recolour step changed nothing are not expanded
+  int* gf0;          // frontier F0 vertices per graph
 };
 
 // ---------------------------------------------------------------------
@@ -391,6 +397,7 @@ struct PushBuf {
 __device__ __forceinline__ void flush(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int k) {
   const int u = lane_id() < k ? pb.buf[lane_id()] : -1;
   __syncwarp();
+  if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
   warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CH, &E.st->status);
   // keep the remainder at the front
   const int rest = pb.cnt - k;
@@ -419,6 +426,7 @@ __device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, 
 __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
   const int v = un.x;
+  if (E.gskip && ld_cg(&E.gskip[E.gid[v]]) == 0) return;  // its graph has stopped
   const int L = g.len[v];
   const long long o = g.off[v];
   const int s_lo = un.y * E.CH;
@@ -467,8 +475,9 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
                               const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
   const long long idx = b * 32 + lane_id();
-  const bool valid = idx < cA;
+  bool valid = idx < cA;
   const int v = valid ? fq.itemsA[idx] : 0;
+  if (valid && E.gskip && ld_cg(&E.gskip[E.gid[v]]) == 0) valid = false;  // its graph has stopped
   const int L = valid ? g.len[v] : 0;
   const long long o = valid ? g.off[v] : 0;
   const int cv = valid ? (g.color[v] & kColorMask) : 0;
@@ -575,7 +584,10 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           const int nc = ld_cg(&E.p.ncolor[v]);
           const int oc = ld_cg(g.color + v) & kColorMask;
           if (E.variant == DC_HI) g.prev[v] = oc;
-          if (nc != oc) changed = true;
+          if (nc != oc) {
+            changed = true;
+            if (E.gchg) atomicAdd(&E.gchg[E.gid[v]], 1);
+          }
           g.color[v] = nc;  // also clears the frontier mark
           cmax_local = max(cmax_local, nc);
           break;
@@ -612,6 +624,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
     }
     if (f0) {
       const bool claim = push >= 0 && mark_bit(E.p.bmB, push);
+      if (claim && E.gf0) atomicAdd(&E.gf0[E.gid[push]], 1);
       warp_push(*f0, f0c, g.len, claim ? push : -1, true, M_MEX_ALL, E.CH, &E.st->status);
     }
   }
@@ -636,6 +649,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.variant = p.variant;
   E.CH = p.unit_slots;
   E.my_scanned = 0;
+  E.gid = p.gid;
+  E.gpush = nullptr;
+  E.gchg = nullptr;
+  E.gskip = nullptr;
+  E.gf0 = p.gid ? p.gf0 : nullptr;
   DevState* st = p.st;
   const GraphDev& g = E.g;
   unsigned bar = 0;
@@ -766,6 +784,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   // F0 is complete: release its marks so the loop can mark into bmB.
   phase_commit(E, B0, &st->q[Q_LOOP0], C_CLEAR_B, nullptr, nullptr, gwarp, nwarps, nullptr,
                nullptr);
+  if (p.gid) {
+    // a graph whose seeding recoloured nothing never enters the loop
+    for (long long gg = gtid; gg < p.ngraphs; gg += gthreads) p.gstate[gg] = ld_cg(&p.gf0[gg]) > 0 ? 1 : 2;
+  }
   if (!grid_sync(st, bar)) return;
   lap(0);
 
@@ -792,6 +814,27 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         z->countU = 0;
         z->masks = 0;
       }
+      const int ring = (int)(it & 1);
+      if (p.gid) {
+        int* cur = p.gcnt + (long long)ring * p.ngraphs;
+        int* prv = p.gcnt + (long long)(ring ^ 1) * p.ngraphs;
+        if (p.variant == DC_HB) {
+          // graphs with no colour change in the previous iteration are done
+          // (the reference's loop would have ended for them)
+          if (it > 1) {
+            for (long long gg = gtid; gg < p.ngraphs; gg += gthreads)
+              if (p.gstate[gg] == 1 && ld_cg(&prv[gg]) == 0) {
+                p.gstate[gg] = 2;
+                p.giters[gg] = (int)(it - 1);
+              }
+          }
+          E.gskip = it > 1 ? prv : nullptr;
+          E.gpush = nullptr;
+        } else {
+          E.gpush = cur;
+          E.gskip = nullptr;
+        }
+      }
       phase_expand(E, sh, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
       ++ps;
       if (!grid_sync(st, bar)) return;
@@ -801,6 +844,19 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       if (p.variant == DC_HI && nq == 0) break;
       // R
       if (leader) st->chg[(it + 1) & 1] = 0;
+      if (p.gid) {
+        int* cur = p.gcnt + (long long)ring * p.ngraphs;
+        int* nxt = p.gcnt + (long long)(ring ^ 1) * p.ngraphs;
+        for (long long gg = gtid; gg < p.ngraphs; gg += gthreads) {
+          // HI: a running graph whose next frontier is empty is done
+          if (p.variant == DC_HI && p.gstate[gg] == 1 && ld_cg(&cur[gg]) == 0) {
+            p.gstate[gg] = 2;
+            p.giters[gg] = (int)it;
+          }
+          nxt[gg] = 0;  // next iteration's counters (last read before this phase)
+        }
+        E.gchg = p.variant == DC_HB ? cur : nullptr;
+      }
       phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
       ++ps;
       if (!grid_sync(st, bar)) return;
@@ -813,6 +869,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       if (p.variant == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;
       fs = ns;
       fb = nb;
+    }
+    if (p.gid) {
+      // graphs still running stop with the union's last iteration
+      for (long long gg = gtid; gg < p.ngraphs; gg += gthreads)
+        if (p.gstate[gg] == 1) p.giters[gg] = (int)it;
     }
     if (leader) {
       st->iterations = (unsigned long long)it;

@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       }
       unsigned long long k0 = SENT, k1 = SENT;
       if (op == 0 || op == 1) {
-        if (a < 0 || a >= g.n || b < 0 || b >= g.n || a == b) {
+        if (a < 0 || a >= g.n || b < 0 || b >= g.n || a == b || (p.gid && p.gid[a] != p.gid[b])) {
           atomicOr(&st->status, ST_INVAL);
         } else {
           k0 = make_key(a, b, op, B);

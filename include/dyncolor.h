@@ -153,6 +153,20 @@ dc_status dc_neighbors(dc_ctx* ctx, int32_t v, int32_t* out, int32_t cap, int32_
 
 dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info);
 
+/* Batched mode (no counterpart in the reference, which runs one graph per
+ * process): declares the loaded graph to be the disjoint union of ngraphs
+ * independent graphs, graph g owning vertices [first[g], first[g+1])
+ * (first[0] = 0, first[ngraphs] = n).  DC_E_INVAL if an edge joins two
+ * graphs.  Afterwards every batch is applied to all graphs in the same
+ * launches, each graph exactly as if it were recoloured alone: HB stops
+ * expanding a graph as soon as one of its recolour steps changes nothing,
+ * and change lines that join two graphs are rejected. */
+dc_status dc_partition_set(dc_ctx* ctx, int32_t ngraphs, const int32_t* first);
+
+/* Batched mode: loop iterations each graph ran in the last batch (what a
+ * separate run of that graph would report). */
+dc_status dc_graph_iterations(dc_ctx* ctx, int64_t* out, int32_t ngraphs);
+
 /* Re-packs the adjacency (drops tombstones, re-applies slack). */
 dc_status dc_compact(dc_ctx* ctx);
 
