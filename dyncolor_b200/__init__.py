@@ -48,7 +48,8 @@ class Options(C.Structure):
         ("blocks_per_sm", C.c_int32),
         ("reserve_slots", C.c_int64),
         ("unit_slots", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("cuda_graph", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -170,7 +171,7 @@ class Context:
 
     def __init__(self, variant: int = HI, device: int = 0, iter_cap: int = 0, slack: float = 0.0,
                  blocks_per_sm: int = 0, unit_slots: int = 0, stream: int | None = None,
-                 reserve_slots: int = 0):
+                 reserve_slots: int = 0, cuda_graph: bool = False):
         L = lib()
         opt = Options()
         L.dc_options_default(C.byref(opt))
@@ -184,6 +185,7 @@ class Context:
         if unit_slots:
             opt.unit_slots = int(unit_slots)
         opt.reserve_slots = int(reserve_slots)
+        opt.cuda_graph = 1 if cuda_graph else 0
         opt.stream = stream
         h = C.c_void_p()
         rc = L.dc_create(C.byref(h), C.byref(opt))

@@ -28,9 +28,16 @@ class BatchedContext:
         first[1:] = np.cumsum(sizes)
         if first[-1] >= 2**31:
             raise ValueError("the union exceeds 2^31 vertices")
-        a = np.concatenate([np.asarray(x, np.int64) + first[i] for i, (_, x, _) in enumerate(graphs)])
-        b = np.concatenate([np.asarray(y, np.int64) + first[i] for i, (_, _, y) in enumerate(graphs)])
-        self.ctx.load_edges(int(first[-1]), a.astype(np.int32), b.astype(np.int32))
+        m = sum(len(x) for _, x, _ in graphs)
+        a = np.empty(m, dtype=np.int32)
+        b = np.empty(m, dtype=np.int32)
+        at = 0
+        for i, (_, x, y) in enumerate(graphs):
+            np.add(x, np.int32(first[i]), out=a[at:at + len(x)], casting="unsafe")
+            np.add(y, np.int32(first[i]), out=b[at:at + len(y)], casting="unsafe")
+            at += len(x)
+        self.ctx.load_edges(int(first[-1]), a, b)
+        del a, b
         self.first = first.astype(np.int32)
         self.ctx.set_partition(self.first)
 

@@ -86,6 +86,13 @@ struct dc_ctx {
 
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
 
+  // captured batch graph
+  cudaGraph_t cgraph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  long long graph_key[5] = {0, 0, 0, 0, 0};
+  long long* h_k = nullptr;  // pinned line count for the captured graph
+  bool last_graph = false;   // the last batch ran from the captured graph
+
   // batched mode: disjoint union of ngraphs graphs
   int ngraphs = 0;
   int* first = nullptr;   // ngraphs + 1
@@ -404,34 +411,100 @@ dc_status repack(dc_ctx* ctx, long long new_cap) {
 }
 
 // Runs one batch (or a load) already resident on the device.
+// Enqueues one attempt of a batch (or load) on the context's stream, ending
+// with the copy of the device state into pinned host memory.  k_dev, when
+// set, makes the kernels read the line count from device memory, so a
+// captured graph of this sequence serves every batch.
+dc_status enqueue_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int* lb, long long k,
+                        bool recolor, const long long* k_dev) {
+  dc_status s;
+  const bool events = k_dev == nullptr;  // events recorded inside a captured graph cannot be timed
+  if (events) DC_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  if ((s = reset_state(ctx)) != DC_OK) return s;
+  StructParams sp = struct_params(ctx, d_ch, la, lb, k);
+  sp.k_dev = k_dev;
+  DC_CK(launch_struct(sp, ctx->grid_struct, ctx->stream));
+  if (events) DC_CK(cudaEventRecord(ctx->evm, ctx->stream));
+  if (recolor) {
+    if (ctx->ngraphs > 0) {
+      const size_t G = (size_t)ctx->ngraphs;
+      DC_CK(cudaMemsetAsync(ctx->gcnt, 0, 2 * G * sizeof(int), ctx->stream));
+      DC_CK(cudaMemsetAsync(ctx->gf0, 0, G * sizeof(int), ctx->stream));
+      DC_CK(cudaMemsetAsync(ctx->giters, 0, G * sizeof(int), ctx->stream));
+      DC_CK(cudaMemsetAsync(ctx->gstate, 0, G * sizeof(int), ctx->stream));
+    }
+    DC_CK(cudaMemcpyAsync(&ctx->st->pre_status, &ctx->st->status, sizeof(unsigned),
+                          cudaMemcpyDeviceToDevice, ctx->stream));
+    // fresh grid barrier and work counters for the second cooperative launch
+    const size_t b0 = offsetof(DevState, bar_arrived);
+    const size_t b1 = offsetof(DevState, wctr) + sizeof(((DevState*)nullptr)->wctr);
+    DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
+    RecolorParams rp = recolor_params(ctx, d_ch, k);
+    rp.k_dev = k_dev;
+    DC_CK(launch_recolor(rp, ctx->grid_recolor, ctx->stream));
+  }
+  if (events) DC_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  DC_CK(cudaMemcpyAsync(ctx->h_st, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+  return DC_OK;
+}
+
+void drop_graph(dc_ctx* ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->cgraph) cudaGraphDestroy(ctx->cgraph);
+  ctx->gexec = nullptr;
+  ctx->cgraph = nullptr;
+}
+
+// Captures the batch sequence (lines in ctx->d_ch, count in st->batch_k)
+// into a CUDA graph; recaptured whenever a buffer it names was reallocated.
+dc_status ensure_graph(dc_ctx* ctx) {
+  const long long key[5] = {ctx->kcap, ctx->k_pool_cap, ctx->rc_pool_cap, ctx->ngraphs,
+                            (long long)(uintptr_t)ctx->d_ch};
+  if (ctx->gexec && std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) return DC_OK;
+  drop_graph(ctx);
+  DC_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  dc_status s = enqueue_batch(ctx, ctx->d_ch, nullptr, nullptr, 0, true, &ctx->st->batch_k);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (s != DC_OK) {
+    if (g) cudaGraphDestroy(g);
+    return s;
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, "cudaStreamEndCapture", e);
+  ctx->cgraph = g;
+  e = cudaGraphInstantiate(&ctx->gexec, g, 0);
+  if (e != cudaSuccess) {
+    drop_graph(ctx);
+    return cuda_fail(ctx, "cudaGraphInstantiate", e);
+  }
+  std::memcpy(ctx->graph_key, key, sizeof(key));
+  return DC_OK;
+}
+
+// Runs one batch (or a load) already resident on the device.
 dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int* lb, long long k,
                     bool recolor, dc_stats* out) {
   dc_status s;
   if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
   if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
-  DC_CK(cudaEventRecord(ctx->ev0, ctx->stream));
   for (int attempt = 0;; ++attempt) {
-    if ((s = reset_state(ctx)) != DC_OK) return s;
-    DC_CK(launch_struct(struct_params(ctx, d_ch, la, lb, k), ctx->grid_struct, ctx->stream));
-    DC_CK(cudaEventRecord(ctx->evm, ctx->stream));
-    if (recolor) {
-      if (ctx->ngraphs > 0) {
-        const size_t G = (size_t)ctx->ngraphs;
-        DC_CK(cudaMemsetAsync(ctx->gcnt, 0, 2 * G * sizeof(int), ctx->stream));
-        DC_CK(cudaMemsetAsync(ctx->gf0, 0, G * sizeof(int), ctx->stream));
-        DC_CK(cudaMemsetAsync(ctx->giters, 0, G * sizeof(int), ctx->stream));
-        DC_CK(cudaMemsetAsync(ctx->gstate, 0, G * sizeof(int), ctx->stream));
-      }
-      DC_CK(cudaMemcpyAsync(&ctx->st->pre_status, &ctx->st->status, sizeof(unsigned),
-                            cudaMemcpyDeviceToDevice, ctx->stream));
-      // fresh grid barrier and work counters for the second cooperative launch
-      const size_t b0 = offsetof(DevState, bar_arrived);
-      const size_t b1 = offsetof(DevState, wctr) + sizeof(((DevState*)nullptr)->wctr);
-      DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
-      DC_CK(launch_recolor(recolor_params(ctx, d_ch, k), ctx->grid_recolor, ctx->stream));
+    const bool graph = ctx->opt.cuda_graph && recolor && attempt == 0;
+    ctx->last_graph = graph;
+    if (graph) {
+      if (d_ch != ctx->d_ch)
+        DC_CK(cudaMemcpyAsync(ctx->d_ch, d_ch, (size_t)k * sizeof(dc_change), cudaMemcpyDeviceToDevice,
+                              ctx->stream));
+      if ((s = ensure_graph(ctx)) != DC_OK) return s;
+      *ctx->h_k = k;
+      DC_CK(cudaEventRecord(ctx->ev0, ctx->stream));
+      DC_CK(cudaMemcpyAsync(&ctx->st->batch_k, ctx->h_k, sizeof(long long), cudaMemcpyHostToDevice,
+                            ctx->stream));
+      DC_CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+      DC_CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    } else {
+      if ((s = enqueue_batch(ctx, d_ch, la, lb, k, recolor, nullptr)) != DC_OK) return s;
     }
-    DC_CK(cudaEventRecord(ctx->ev1, ctx->stream));
-    if ((s = read_state(ctx)) != DC_OK) return s;
+    DC_CK(cudaStreamSynchronize(ctx->stream));
     const unsigned stt = ctx->h_st->status;
     if ((stt & ST_POOL) && !(stt & (ST_OVERFLOW | ST_TIMEOUT | ST_INVAL)) && attempt < 4) {
       const long long grow = std::max<long long>(ctx->pool_cap, 4ll * k + 4096);
@@ -444,9 +517,17 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   }
   const DevState& h = *ctx->h_st;
   float ms = 0.f, ms_s = 0.f, ms_r = 0.f;
-  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-  cudaEventElapsedTime(&ms_s, ctx->ev0, ctx->evm);
-  cudaEventElapsedTime(&ms_r, ctx->evm, ctx->ev1);
+  // (a failure here only loses the timing; clear it so no later call sees it)
+  if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) != cudaSuccess) ms = -1.f;
+  if (ctx->last_graph) {
+    // launch split from the kernels' own %globaltimer stamps
+    ms_s = h.t_struct[1] > h.t_struct[0] ? (float)((h.t_struct[1] - h.t_struct[0]) * 1e-6) : -1.f;
+    ms_r = h.t_recolor[1] > h.t_recolor[0] ? (float)((h.t_recolor[1] - h.t_recolor[0]) * 1e-6) : -1.f;
+  } else {
+    if (cudaEventElapsedTime(&ms_s, ctx->ev0, ctx->evm) != cudaSuccess) ms_s = -1.f;
+    if (cudaEventElapsedTime(&ms_r, ctx->evm, ctx->ev1) != cudaSuccess) ms_r = -1.f;
+  }
+  cudaGetLastError();
   dc_status rc = DC_OK;
   if (h.status & ST_INVAL)
     rc = fail(ctx, DC_E_INVAL, "change line with a vertex id outside [0,n) or a self-loop");
@@ -570,6 +651,7 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   if (cudaMallocHost((void**)&ctx->h_st, sizeof(DevState)) != cudaSuccess) return bail(DC_E_NOMEM);
   if (cudaMalloc((void**)&ctx->d_scalar, 16) != cudaSuccess) return bail(DC_E_NOMEM);
   if (cudaMallocHost((void**)&ctx->h_scalar, 16) != cudaSuccess) return bail(DC_E_NOMEM);
+  if (cudaMallocHost((void**)&ctx->h_k, sizeof(long long)) != cudaSuccess) return bail(DC_E_NOMEM);
   *out = ctx;
   return DC_OK;
 }
@@ -577,6 +659,7 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
 void dc_destroy(dc_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   free_batch_scratch(ctx);
   for (int b = 0; b < 3; ++b) {
@@ -607,6 +690,8 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->d_scalar);
   if (ctx->h_st) cudaFreeHost(ctx->h_st);
   if (ctx->h_scalar) cudaFreeHost(ctx->h_scalar);
+  if (ctx->h_k) cudaFreeHost(ctx->h_k);
+  drop_graph(ctx);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   if (ctx->evm) cudaEventDestroy(ctx->evm);
@@ -623,6 +708,7 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
     if (a[i] < 0 || a[i] >= n || b[i] < 0 || b[i] >= n || a[i] == b[i])
       return fail(ctx, DC_E_INVAL, "edge " + std::to_string(i) + " has an id outside [0,n) or is a self-loop");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   ctx->n = n;
   ctx->key_bits = key_bits_for(n);
   const long long nn = std::max(n, 1);
@@ -648,16 +734,22 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
   if ((s = dalloc(ctx, &ctx->adj, pool, "adjacency pool")) != DC_OK) return s;
   DC_CK(cudaMemsetAsync(ctx->st, 0, sizeof(DevState), ctx->stream));
   if (m > 0) {
+    // Large edge lists go in pieces so the sort scratch stays bounded; every
+    // piece is an insertion batch into the rows built so far.
+    const long long piece = std::min<long long>(m, kLoadPiece);
     int* da = nullptr;
     int* db = nullptr;
-    if ((s = dalloc(ctx, &da, m, "load pairs")) != DC_OK) return s;
-    if ((s = dalloc(ctx, &db, m, "load pairs")) != DC_OK) {
+    if ((s = dalloc(ctx, &da, piece, "load pairs")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &db, piece, "load pairs")) != DC_OK) {
       dfree(ctx, &da);
       return s;
     }
-    cudaMemcpyAsync(da, a, (size_t)m * 4, cudaMemcpyHostToDevice, ctx->stream);
-    cudaMemcpyAsync(db, b, (size_t)m * 4, cudaMemcpyHostToDevice, ctx->stream);
-    s = run_batch(ctx, nullptr, da, db, m, false, nullptr);
+    for (long long at = 0; at < m && s == DC_OK; at += piece) {
+      const long long len = std::min<long long>(piece, m - at);
+      cudaMemcpyAsync(da, a + at, (size_t)len * 4, cudaMemcpyHostToDevice, ctx->stream);
+      cudaMemcpyAsync(db, b + at, (size_t)len * 4, cudaMemcpyHostToDevice, ctx->stream);
+      s = run_batch(ctx, nullptr, da, db, len, false, nullptr);
+    }
     dfree(ctx, &da);
     dfree(ctx, &db);
     // load-sized scratch is not needed by typical batches
@@ -677,6 +769,7 @@ dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
     if (colors[v] < 0 || colors[v] > kColorMask)
       return fail(ctx, DC_E_INVAL, "colour outside [0, 2^30) at vertex " + std::to_string(v));
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   if (n > 0) DC_CK(cudaMemcpyAsync(ctx->color, colors, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
   DC_CK(launch_color_max(graph_dev(ctx), ctx->st, ctx->stream));
   DC_CK(cudaStreamSynchronize(ctx->stream));
@@ -690,6 +783,7 @@ dc_status dc_apply_batch(dc_ctx* ctx, const dc_change* changes, int64_t k, dc_st
   if (out) std::memset(out, 0, sizeof(*out));
   if (k == 0) return DC_OK;
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   dc_status s;
   if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
   DC_CK(cudaMemcpyAsync(ctx->d_ch, changes, (size_t)k * sizeof(dc_change), cudaMemcpyHostToDevice,
@@ -704,6 +798,7 @@ dc_status dc_apply_batch_device(dc_ctx* ctx, const dc_change* d_changes, int64_t
   if (out) std::memset(out, 0, sizeof(*out));
   if (k == 0) return DC_OK;
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   return run_batch(ctx, d_changes, nullptr, nullptr, k, true, out);
 }
 
@@ -711,6 +806,7 @@ dc_status dc_colors_read(dc_ctx* ctx, int32_t* out, int32_t n) {
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   if (n != ctx->n || (n > 0 && !out)) return fail(ctx, DC_E_INVAL, "output size differs from n");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   if (n > 0) DC_CK(cudaMemcpyAsync(out, ctx->color, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
   DC_CK(cudaStreamSynchronize(ctx->stream));
   return DC_OK;
@@ -727,6 +823,7 @@ dc_status dc_prop_read(dc_ctx* ctx, int32_t* out, int32_t n) {
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   if (n != ctx->n || (n > 0 && !out)) return fail(ctx, DC_E_INVAL, "output size differs from n");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   if (n > 0) DC_CK(cudaMemcpyAsync(out, ctx->prop, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
   DC_CK(cudaStreamSynchronize(ctx->stream));
   return DC_OK;
@@ -736,6 +833,7 @@ dc_status dc_validate(dc_ctx* ctx, int64_t* conflicts) {
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   if (!conflicts) return DC_E_INVAL;
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   DC_CK(launch_validate(graph_dev(ctx), ctx->d_scalar, ctx->stream));
   DC_CK(cudaMemcpyAsync(ctx->h_scalar, ctx->d_scalar, 8, cudaMemcpyDeviceToHost, ctx->stream));
   DC_CK(cudaStreamSynchronize(ctx->stream));
@@ -747,6 +845,7 @@ dc_status dc_neighbors(dc_ctx* ctx, int32_t v, int32_t* out, int32_t cap, int32_
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   if (v < 0 || v >= ctx->n || !deg || (cap > 0 && !out)) return fail(ctx, DC_E_INVAL, "bad vertex");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   long long o = 0;
   int L = 0;
   DC_CK(cudaMemcpyAsync(&o, ctx->off + v, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -771,6 +870,7 @@ dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info) {
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   if (!info) return DC_E_INVAL;
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   DC_CK(launch_count_live(graph_dev(ctx), ctx->d_scalar, ctx->stream));
   DC_CK(cudaMemcpyAsync(ctx->h_scalar, ctx->d_scalar, 8, cudaMemcpyDeviceToHost, ctx->stream));
   DC_CK(cudaMemcpyAsync(ctx->h_scalar + 1, &ctx->st->pool_used, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -786,6 +886,7 @@ dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info) {
 dc_status dc_compact(dc_ctx* ctx) {
   if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   dc_status s = repack(ctx, ctx->pool_cap);
   if (s != DC_OK) return s;
   if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
@@ -801,6 +902,7 @@ dc_status dc_partition_set(dc_ctx* ctx, int32_t ngraphs, const int32_t* first) {
   for (int32_t g = 0; g < ngraphs; ++g)
     if (first[g + 1] < first[g]) return fail(ctx, DC_E_INVAL, "partition offsets must not decrease");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   const long long G = ngraphs;
   dc_status s;
   if ((s = dalloc(ctx, &ctx->first, G + 1, "partition offsets")) != DC_OK) return s;
@@ -827,6 +929,7 @@ dc_status dc_graph_iterations(dc_ctx* ctx, int64_t* out, int32_t ngraphs) {
   if (ctx->ngraphs == 0) return fail(ctx, DC_E_STATE, "no partition set");
   if (ngraphs != ctx->ngraphs || !out) return fail(ctx, DC_E_INVAL, "output size differs from the partition");
   cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
   std::vector<int> tmp((size_t)ngraphs);
   DC_CK(cudaMemcpyAsync(tmp.data(), ctx->giters, (size_t)ngraphs * sizeof(int), cudaMemcpyDeviceToHost,
                         ctx->stream));

@@ -30,6 +30,7 @@ constexpr unsigned kMarkBit = 1u << 30;
 constexpr int kColorMask = (1 << 30) - 1;
 constexpr int kNumQueues = 6;       // logical queue counter slots
 constexpr int kUnitSlotsDefault = 2048;  // adjacency slots per warp work unit
+constexpr long long kLoadPiece = 1ll << 27;  // edge pairs per structural launch of a graph load
 constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
 
 // Logical queue counter slots.
@@ -49,6 +50,7 @@ struct DevState {
   int cmax;                        // upper bound of every colour value
   int pad0;
   unsigned long long pool_used;    // adjacency pool slots handed out
+  long long batch_k;               // line count, read by kernels of a captured batch graph
   unsigned long long pool_used_start;
   // ---- cleared before every kernel launch (bar_arrived .. wctr) ----
   unsigned bar_arrived;
@@ -76,6 +78,8 @@ struct DevState {
   unsigned long long edges_deleted;
   unsigned long long rows_relocated;
   unsigned long long slots_read;      // adjacency entries the kernels actually read
+  unsigned long long t_struct[2];     // %globaltimer at the start and end of the structural launch
+  unsigned long long t_recolor[2];    // same for the recolour launch
   unsigned long long phase_ns[6];     // recolour launch: seeding, find-eligible, mex, commit, 2 spare
 };
 
@@ -106,6 +110,7 @@ struct StructParams {
   const int* la;         // graph-load pairs when ch == NULL
   const int* lb;
   long long k;           // number of lines
+  const long long* k_dev;  // when set, the line count is read from here (captured graphs)
   float slack;
   unsigned long long* keysA;  // 2k
   unsigned long long* keysB;  // 2k
@@ -138,6 +143,7 @@ struct RecolorParams {
   GraphDev g;
   const dc_change* ch;
   long long k;
+  const long long* k_dev;  // when set, the line count is read from here (captured graphs)
   int variant;
   int unit_slots;        // slots per work unit (multiple of 128)
   long long iter_cap;

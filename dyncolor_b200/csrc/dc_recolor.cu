@@ -669,6 +669,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   // Phase timer: CTA 0 thread 0 reads %globaltimer after each barrier and
   // charges the elapsed time to the phase kind that just ended.
   unsigned long long t_last = leader ? globaltimer_ns() : 0ull;
+  if (leader) st->t_recolor[0] = t_last;
   unsigned long long acc[6] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
   auto lap = [&](int kind) {
     if (leader) {
@@ -681,6 +682,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   const QueueBufs& B1 = p.qb[1];  // odd loop queues, HI insertion targets
   const QueueBufs& B2 = p.qb[2];  // seeding sets
   const dc_change* ch = p.ch;
+  const long long K = p.k_dev ? *p.k_dev : p.k;
   // The structural launch failed (invalid line, pool exhausted, ...): the
   // batch is not applied.  Uniform: nothing writes pre_status here.
   if (ld_cg(&st->pre_status) != 0u) return;
@@ -688,10 +690,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   // ======================= seeding =======================
   if (p.variant == DC_HI) {
     // D1: deletion targets (and remember which insertions had equal colours)
-    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+    for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
       int t = -1;
-      if (i < p.k) {
+      if (i < K) {
         const dc_change c = ch[i];
         if (c.inst == 0) {
           t = g.color[c.node1] > g.color[c.node2] ? c.node1 : c.node2;
@@ -711,10 +713,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
                  &st->seed_targets, nullptr);
     if (!grid_sync(st, bar)) return;
     // I1: insertions still monochromatic -> both endpoints
-    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+    for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
       int a = -1, b = -1;
-      if (i < p.k && p.lflag[i]) {
+      if (i < K && p.lflag[i]) {
         const dc_change c = ch[i];
         if (g.color[c.node1] == g.color[c.node2]) {
           a = c.node1;
@@ -733,10 +735,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     ++ps;
     if (!grid_sync(st, bar)) return;
     // I3: targets; release the endpoint set
-    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+    for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
       int t = -1;
-      if (i < p.k && p.lflag[i] == 2) {
+      if (i < K && p.lflag[i] == 2) {
         const dc_change c = ch[i];
         t = ld_cg(&p.sat[c.node1]) < ld_cg(&p.sat[c.node2]) ? c.node1 : c.node2;
       }
@@ -756,10 +758,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     if (!grid_sync(st, bar)) return;
   } else {
     // H1: endpoints of equal-colour insertions and of all deletions
-    for (long long i0 = gwarp * 32; i0 < p.k; i0 += nwarps * 32) {
+    for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
       int a = -1, b = -1;
-      if (i < p.k) {
+      if (i < K) {
         const dc_change c = ch[i];
         if (c.inst == 0 || (c.inst == 1 && g.color[c.node1] == g.color[c.node2])) {
           a = c.node1;
@@ -878,6 +880,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     if (leader) {
       st->iterations = (unsigned long long)it;
       for (int i = 0; i < 6; ++i) st->phase_ns[i] = acc[i];
+      st->t_recolor[1] = globaltimer_ns();
     }
   }
   const long long sc = warp_sum_ll(E.my_scanned);

@@ -77,13 +77,16 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
   const long long gtid = (long long)blockIdx.x * blockDim.x + tid;
   const long long gwarp = gtid >> 5, nwarps = gthreads >> 5;
   const unsigned long long SENT = (1ull << (2 * B + 1)) - 1ull;
-  const long long N = 2 * p.k;
+  const long long K = p.k_dev ? *p.k_dev : p.k;
+  const long long N = 2 * K;
   unsigned bar = 0;
+  const bool leader = blockIdx.x == 0 && tid == 0;
+  if (leader) st->t_struct[0] = globaltimer_ns();
 
   // ---------------- S0: keys + validation ----------------
   {
     int nv = 0;
-    for (long long i = gtid; i < p.k; i += gthreads) {
+    for (long long i = gtid; i < K; i += gthreads) {
       int a, b, op;
       if (p.ch) {
         const dc_change c = p.ch[i];
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
   {
     const long long ND = min((long long)ld_cg(&st->ndel), N);
     for (long long d = gtid; d < ND; d += gthreads) g.adj[p.delpos[d]] = kTomb;
-    for (long long i = gtid; i < p.k; i += gthreads) {
+    for (long long i = gtid; i < K; i += gthreads) {
       int a, b, op;
       if (p.ch) {
         const dc_change c = p.ch[i];
@@ -505,6 +508,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
     }
     g.live[r] = p.tnlive[t];
   }
+  if (leader) st->t_struct[1] = globaltimer_ns();
 }
 
 cudaError_t launch_struct(const StructParams& p, int grid, cudaStream_t s) {

@@ -75,7 +75,8 @@ typedef struct {
   int32_t blocks_per_sm; /* persistent-kernel CTAs per SM; 0: from occupancy */
   int64_t reserve_slots; /* initial adjacency pool size hint in slots; 0: automatic */
   int32_t unit_slots;    /* adjacency slots per warp work unit (multiple of 128); 0: 2048 */
-  int32_t reserved[7];
+  int32_t cuda_graph;    /* 1: replay each batch's launches from a captured CUDA graph */
+  int32_t reserved[6];
 } dc_options;
 
 typedef struct {

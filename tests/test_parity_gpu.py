@@ -268,3 +268,21 @@ def test_device_resident_batch_entry_point():
     d = torch.from_numpy(ch.view(np.int32).reshape(-1, 3).copy()).cuda()
     sg = ctx.apply_batch_device(d.data_ptr(), len(ch))
     check_same(ctx, g, sg, so)
+
+
+@pytest.mark.parametrize("variant,ov", VARIANTS)
+def test_cuda_graph_replay_matches_oracle(variant, ov):
+    """Batches replayed from a captured CUDA graph: the line count changes
+    every batch (read from device memory), the scratch grows (recapture) and
+    a tiny slack forces pool growth (direct-path retry)."""
+    n, a, b = rmat_graph(12, 8, seed=31)
+    col = dc.greedy_color(n, a, b)
+    es = dc.EdgeSet(n, a, b)
+    ctx = gpu_ctx(variant, n, a, b, col, cuda_graph=True, slack=1.01)
+    g = oracle_graph(n, a, b, col)
+    for i, k in enumerate((50, 600, 10, 3000, 700, 1)):
+        ch = es.sample_batch(k // 2, k - k // 2, seed=40 + i)
+        rc, so = g.apply_batch(ch, ov, po.SNAPSHOT)
+        sg = ctx.apply_batch(to_dc_changes(ch))
+        check_same(ctx, g, sg, so)
+    ctx.close()
