@@ -14,139 +14,13 @@
 #include <vector>
 
 #include "../../include/dyncolor.h"
-#include "dc_internal.h"
+#include "dc_ctx.h"
 
 using namespace dc;
 
-struct dc_ctx {
-  dc_options opt{};
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  int sms = 0;
-  int grid_struct = 0;
-  int grid_recolor = 0;
-  std::string err;
-  long long bytes = 0;
 
-  // graph
-  int n = -1;
-  int key_bits = 1;
-  long long pool_cap = 0;
-  long long* off = nullptr;
-  int* len = nullptr;
-  int* cap = nullptr;
-  int* live = nullptr;
-  int* adj = nullptr;
-  int* color = nullptr;
-  int* prev = nullptr;
-  int* prop = nullptr;
-  DevState* st = nullptr;
-  DevState* h_st = nullptr;  // pinned
-  unsigned long long* d_scalar = nullptr;
-  unsigned long long* h_scalar = nullptr;  // pinned
-
-  // recolour scratch (sized by n and pool_cap)
-  long long rc_pool_cap = -1;
-  QueueBufs qb[3]{};
-  unsigned* bmA = nullptr;
-  unsigned* bmB = nullptr;
-  unsigned* bmC = nullptr;
-  int* ncolor = nullptr;
-  int* sat = nullptr;
-
-  // batch scratch (sized by k and pool_cap)
-  long long kcap = 0;
-  long long k_pool_cap = -1;
-  dc_change* d_ch = nullptr;
-  unsigned char* lflag = nullptr;
-  unsigned long long* keysA = nullptr;
-  unsigned long long* keysB = nullptr;
-  unsigned long long* net = nullptr;
-  int* tof = nullptr;
-  unsigned char* present = nullptr;
-  int* rank = nullptr;
-  int* tbeg = nullptr;
-  int* trow = nullptr;
-  int* rowdel = nullptr;
-  int* tins = nullptr;
-  long long* tnoff = nullptr;
-  int* tncap = nullptr;
-  int* tnlive = nullptr;
-  int* trel = nullptr;
-  int* cursor = nullptr;
-  long long* delpos = nullptr;
-  int2* units = nullptr;
-  int2* relunits = nullptr;
-  long long cap_units = 0;
-  long long cap_rel = 0;
-  unsigned* hist = nullptr;
-  unsigned* dscan = nullptr;
-  unsigned* cta_cnt = nullptr;
-
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evm = nullptr;
-
-  // captured batch graph
-  cudaGraph_t cgraph = nullptr;
-  cudaGraphExec_t gexec = nullptr;
-  long long graph_key[5] = {0, 0, 0, 0, 0};
-  long long* h_k = nullptr;  // pinned line count for the captured graph
-  bool last_graph = false;   // the last batch ran from the captured graph
-
-  // batched mode: disjoint union of ngraphs graphs
-  int ngraphs = 0;
-  int* first = nullptr;   // ngraphs + 1
-  int* gid = nullptr;     // n
-  int* gcnt = nullptr;    // 2 * ngraphs
-  int* gf0 = nullptr;     // ngraphs
-  int* giters = nullptr;  // ngraphs
-  int* gstate = nullptr;  // ngraphs
-};
-
-namespace {
-
-dc_status fail(dc_ctx* c, dc_status s, const std::string& what) {
-  if (c) c->err = what;
-  return s;
-}
-
-dc_status cuda_fail(dc_ctx* c, const char* what, cudaError_t e) {
-  return fail(c, e == cudaErrorMemoryAllocation ? DC_E_NOMEM : DC_E_CUDA,
-              std::string(what) + ": " + cudaGetErrorString(e));
-}
-
-#define DC_CK(call)                                      \
-  do {                                                   \
-    cudaError_t e_ = (call);                             \
-    if (e_ != cudaSuccess) return cuda_fail(ctx, #call, e_); \
-  } while (0)
-
-template <class T>
-dc_status dalloc(dc_ctx* ctx, T** p, long long count, const char* what) {
-  if (*p) {
-    cudaFree(*p);
-    *p = nullptr;
-  }
-  if (count <= 0) count = 1;
-  const size_t bytes = (size_t)count * sizeof(T);
-  cudaError_t e = cudaMalloc((void**)p, bytes);
-  if (e != cudaSuccess) {
-    *p = nullptr;
-    cudaGetLastError();
-    return fail(ctx, DC_E_NOMEM, std::string("cudaMalloc ") + what + " (" + std::to_string(bytes) + " bytes)");
-  }
-  ctx->bytes += (long long)bytes;
-  return DC_OK;
-}
-
-template <class T>
-void dfree(dc_ctx* ctx, T** p) {
-  if (*p) {
-    cudaFree(*p);
-    *p = nullptr;
-  }
-  (void)ctx;
-}
+namespace dc {
+namespace host {
 
 int key_bits_for(int n) {
   int B = 1;
@@ -364,6 +238,8 @@ dc_status read_state(dc_ctx* ctx) {
   return DC_OK;
 }
 
+void drop_graph(dc_ctx* ctx);
+
 // Moves the adjacency into a fresh pool of new_cap slots (tombstones dropped).
 dc_status repack(dc_ctx* ctx, long long new_cap) {
   GraphDev g = graph_dev(ctx);
@@ -407,6 +283,7 @@ dc_status repack(dc_ctx* ctx, long long new_cap) {
   ctx->cap = cap2;
   ctx->adj = adj2;
   ctx->pool_cap = new_cap;
+  drop_graph(ctx);  // a captured batch graph names the old arrays
   return DC_OK;
 }
 
@@ -487,6 +364,7 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   dc_status s;
   if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
   if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+  bool compacted = false;
   for (int attempt = 0;; ++attempt) {
     const bool graph = ctx->opt.cuda_graph && recolor && attempt == 0;
     ctx->last_graph = graph;
@@ -507,7 +385,13 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
     DC_CK(cudaStreamSynchronize(ctx->stream));
     const unsigned stt = ctx->h_st->status;
     if ((stt & ST_POOL) && !(stt & (ST_OVERFLOW | ST_TIMEOUT | ST_INVAL)) && attempt < 4) {
-      const long long grow = std::max<long long>(ctx->pool_cap, 4ll * k + 4096);
+      long long grow = std::max<long long>(ctx->pool_cap, 4ll * k + 4096);
+      if (ctx->max_pool_cap > 0) {
+        // a budgeted pool: grow up to the cap, else compact once in place
+        grow = std::max<long long>(0, std::min(grow, ctx->max_pool_cap - ctx->pool_cap));
+        if (grow == 0 && compacted) break;
+        compacted = compacted || grow == 0;
+      }
       if ((s = repack(ctx, ctx->pool_cap + grow)) != DC_OK) return s;
       if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
       if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
@@ -567,7 +451,10 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
 
 bool ready(dc_ctx* ctx) { return ctx && ctx->n >= 0; }
 
-}  // namespace
+}  // namespace host
+}  // namespace dc
+
+using namespace dc::host;
 
 extern "C" {
 
@@ -703,7 +590,9 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
   if (!ctx) return DC_E_INVAL;
   if (ctx->n >= 0) return fail(ctx, DC_E_STATE, "graph already loaded");
   if (n < 0 || m < 0 || (m > 0 && (!a || !b))) return fail(ctx, DC_E_INVAL, "bad graph arguments");
-  if (m > (1ll << 30)) return fail(ctx, DC_E_INVAL, "more than 2^30 edge lines");
+  // pieces of kLoadPiece lines keep the sort keys and scratch in range; the
+  // pool of 2 * m * slack slots is the only size limit past this one
+  if (m > (1ll << 36)) return fail(ctx, DC_E_INVAL, "more than 2^36 edge lines");
   for (int64_t i = 0; i < m; ++i)
     if (a[i] < 0 || a[i] >= n || b[i] < 0 || b[i] >= n || a[i] == b[i])
       return fail(ctx, DC_E_INVAL, "edge " + std::to_string(i) + " has an id outside [0,n) or is a self-loop");
@@ -730,6 +619,7 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
   const double slack = ctx->opt.slack;
   long long pool = (long long)std::ceil(2.0 * (double)m * slack) + 8ll * nn + 4096;
   pool = std::max<long long>(pool, ctx->opt.reserve_slots);
+  if (ctx->max_pool_cap > 0) pool = ctx->max_pool_cap;  // a budgeted pool takes its whole budget at once
   ctx->pool_cap = pool;
   if ((s = dalloc(ctx, &ctx->adj, pool, "adjacency pool")) != DC_OK) return s;
   DC_CK(cudaMemsetAsync(ctx->st, 0, sizeof(DevState), ctx->stream));

@@ -182,5 +182,12 @@ cudaError_t launch_partition(const GraphDev& g, const int* first, int ngraphs, i
 cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* adj2,
                           long long cap_slots, float slack, unsigned long long* used,
                           unsigned* status, long long* scratch, cudaStream_t s);
+// Resident pool: copy the rows of vertices [v0, v0 + nv) out to / in from a
+// packed buffer (row i at pre[i]), with vertex ids shifted by -base / +base.
+cudaError_t launch_range_gather(const GraphDev& g, int base, int v0, int nv, const long long* pre, int* out,
+                                cudaStream_t s);
+cudaError_t launch_range_scatter(const GraphDev& g, int base, int v0, int nv, const long long* pre, const int* in,
+                                 cudaStream_t s);
+cudaError_t launch_fill(int* p, long long count, int value, cudaStream_t s);
 
 }  // namespace dc

@@ -178,6 +178,50 @@ __global__ void repack_copy_kernel(GraphDev g, const long long* off2, int* adj2,
   }
 }
 
+// Resident pool: rows of vertices [v0, v0 + nv) copied out in row order
+// (tombstones dropped, ids made local by subtracting `base`); row i's live
+// entries land at out[pre[i] ..).  One warp per row.
+__global__ void range_gather_kernel(GraphDev g, int base, int v0, int nv, const long long* pre, int* out) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = gw; i < nv; i += nw) {
+    const long long v = v0 + i;
+    const long long o = g.off[v];
+    const int L = g.len[v];
+    int* dst = out + pre[i];
+    const long long room = pre[i + 1] - pre[i];  // live[v] as the host read it
+    int cur = 0;
+    for (int s0 = 0; s0 < L; s0 += 32) {
+      const int s = s0 + lane_id();
+      const int x = s < L ? g.adj[o + s] : kTomb;
+      const unsigned bal = __ballot_sync(0xffffffffu, x >= 0);
+      const int at = cur + __popc(bal & lanemask_lt());
+      if (x >= 0 && at < room) dst[at] = x - base;
+      cur += __popc(bal);
+    }
+  }
+}
+
+// The inverse: row i (vertex v0 + i, whose off/len were already written)
+// takes in[pre[i] .. pre[i] + len) with `base` added to every id.
+__global__ void range_scatter_kernel(GraphDev g, int base, int v0, int nv, const long long* pre, const int* in) {
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = gw; i < nv; i += nw) {
+    const long long v = v0 + i;
+    const long long o = g.off[v];
+    const int L = g.len[v];
+    const int* src = in + pre[i];
+    for (int s = lane_id(); s < L; s += 32) g.adj[o + s] = src[s] + base;
+  }
+}
+
+__global__ void fill_kernel(int* p, long long count, int value) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    p[i] = value;
+}
+
 }  // namespace
 
 static int misc_grid(long long work, int per_block) {
@@ -233,6 +277,26 @@ cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* ad
   repack_offsets_kernel<<<(unsigned)nb, kMiscThreads, 0, s>>>(g, slack, scratch, off2, cap2);
   repack_copy_kernel<<<misc_grid((long long)g.n * 32, kMiscThreads), kMiscThreads, 0, s>>>(
       g, off2, adj2, cap_slots, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_range_gather(const GraphDev& g, int base, int v0, int nv, const long long* pre, int* out,
+                                cudaStream_t s) {
+  if (nv <= 0) return cudaSuccess;
+  range_gather_kernel<<<misc_grid((long long)nv * 32, kMiscThreads), kMiscThreads, 0, s>>>(g, base, v0, nv, pre, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_range_scatter(const GraphDev& g, int base, int v0, int nv, const long long* pre, const int* in,
+                                 cudaStream_t s) {
+  if (nv <= 0) return cudaSuccess;
+  range_scatter_kernel<<<misc_grid((long long)nv * 32, kMiscThreads), kMiscThreads, 0, s>>>(g, base, v0, nv, pre, in);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill(int* p, long long count, int value, cudaStream_t s) {
+  if (count <= 0) return cudaSuccess;
+  fill_kernel<<<misc_grid(count, kMiscThreads), kMiscThreads, 0, s>>>(p, count, value);
   return cudaGetLastError();
 }
 

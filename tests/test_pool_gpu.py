@@ -1,0 +1,139 @@
+"""Resident pool: graphs spilled to pinned host memory and reloaded, several
+graphs' batches in one launch; every graph ends exactly as when its batches
+are applied alone and in order (colours and loop iterations), checked
+against the CPU oracle."""
+import numpy as np
+import pytest
+
+import dyncolor_b200 as dc
+import pyoracle as po
+from dyncolor_b200.pool import ResidentPool
+from helpers import oracle_graph, to_oracle_changes
+
+pytestmark = pytest.mark.gpu
+
+
+def make_workload(count, seed, rounds=4):
+    rng = np.random.default_rng(seed)
+    graphs, colors, seqs = [], [], []
+    for i in range(count):
+        n = int(rng.integers(300, 3000))
+        m = int(n * float(rng.uniform(4, 16)) / 2)
+        if i % 2 == 0:
+            a, b = dc.rmat(int(np.ceil(np.log2(n))), m, seed=seed * 100 + i, n=n)
+        else:
+            a, b = dc.uniform_pairs(n, m, seed=seed * 100 + i)
+        a, b = dc.dedup(n, a, b)
+        graphs.append((n, a, b))
+        colors.append(dc.greedy_color(n, a, b) if i % 3 else rng.integers(0, 6, n).astype(np.int32))
+        es = dc.EdgeSet(n, a, b)
+        seq = []
+        for r in range(rounds):
+            k = int(rng.integers(1, max(4, m // 3)))
+            kd = min(k // 2, es.size())
+            seq.append(es.sample_batch(kd, k - kd, seed=seed * 1000 + i * 10 + r))
+        seqs.append(seq)
+    return graphs, colors, seqs
+
+
+def oracle_runs(graphs, colors, seqs, ov):
+    """Per graph: the colours after all its batches and each batch's iterations."""
+    out = []
+    for (n, a, b), c, seq in zip(graphs, colors, seqs):
+        o = oracle_graph(n, a, b, c)
+        its = []
+        for ch in seq:
+            rc, so = o.apply_batch(to_oracle_changes(ch), ov, po.SNAPSHOT)
+            assert rc == po.OK
+            its.append(so.iterations)
+        out.append((o.colors(), its))
+    return out
+
+
+@pytest.mark.parametrize("variant,ov", [(dc.HI, po.HI), (dc.HB, po.HB)])
+def test_pool_spill_reload_and_shared_launches_match_alone(variant, ov):
+    graphs, colors, seqs = make_workload(10, seed=3)
+    want = oracle_runs(graphs, colors, seqs, ov)
+    nmax = max(n for n, _, _ in graphs)
+    # room for about three graphs: every launch below forces evictions
+    slots = int(3.2 * max(2 * len(a) for _, a, _ in graphs) * 1.25) + 64 * nmax
+    pool = ResidentPool(variant=variant, vertex_capacity=3 * nmax, pool_slots=slots, max_graphs=16,
+                        unit_slots=256, stage_slots=4096)
+    ids = [pool.add_graph(n, a, b, c) for (n, a, b), c in zip(graphs, colors)]
+    assert ids == list(range(len(graphs)))
+    info = pool.info()
+    assert info["spills"] > 0 and info["resident"] < len(graphs)
+    rng = np.random.default_rng(11)
+    nxt = [0] * len(graphs)
+    its = [[] for _ in graphs]
+    restored = 0
+    while any(nxt[g] < len(seqs[g]) for g in range(len(graphs))):
+        pending = [g for g in range(len(graphs)) if nxt[g] < len(seqs[g])]
+        take = rng.choice(pending, size=min(len(pending), int(rng.integers(1, 3))), replace=False)
+        st, it, rs = pool.apply([(int(g), seqs[g][nxt[g]]) for g in take])
+        restored += int(rs.sum())
+        for j, g in enumerate(take):
+            its[g].append(int(it[j]))
+            nxt[g] += 1
+        if rng.random() < 0.3:
+            pool.spill(int(rng.integers(0, len(graphs))))  # explicit spill, resident or not
+    for g, (cw, iw) in enumerate(want):
+        assert np.array_equal(pool.colors(g), cw), f"graph {g}: colours differ from the oracle"
+        assert its[g] == iw, f"graph {g}: iterations {its[g]}, oracle {iw}"
+    info = pool.info()
+    assert info["restores"] > 0 and restored > 0
+    assert info["pool_slots_used"] <= info["pool_slots"]
+    pool.close()
+
+
+def test_pool_rejects_bad_requests_without_changing_state():
+    graphs, colors, seqs = make_workload(3, seed=4, rounds=1)
+    pool = ResidentPool(vertex_capacity=10_000, pool_slots=1 << 20, max_graphs=4)
+    for (n, a, b), c in zip(graphs, colors):
+        pool.add_graph(n, a, b, c)
+    before = [pool.colors(g) for g in range(3)]
+    n0 = graphs[0][0]
+    bad = dc.as_changes([0], [n0], [1])  # id outside graph 0
+    with pytest.raises(dc.DcError) as e:
+        pool.apply([(1, seqs[1][0]), (0, bad)])
+    assert e.value.status == dc.E_INVAL
+    with pytest.raises(dc.DcError) as e:
+        pool.apply([(1, seqs[1][0]), (1, seqs[1][0])])  # two batches for one graph
+    assert e.value.status == dc.E_INVAL
+    with pytest.raises(dc.DcError) as e:
+        pool.apply([(7, seqs[1][0])])
+    assert e.value.status == dc.E_INVAL
+    for g in range(3):
+        assert np.array_equal(pool.colors(g), before[g])
+    # an empty launch and an empty batch are no-ops
+    st, it, _ = pool.apply([])
+    st, it, _ = pool.apply([(2, np.empty(0, dtype=dc.CHANGE_DTYPE))])
+    assert it[0] == 0 and np.array_equal(pool.colors(2), before[2])
+    # a graph larger than the budget is refused
+    n, a, b = graphs[0]
+    small = ResidentPool(vertex_capacity=n - 1, pool_slots=1 << 16, max_graphs=2)
+    with pytest.raises(dc.DcError) as e:
+        small.add_graph(n, a, b, colors[0])
+    assert e.value.status == dc.E_NOMEM
+    small.close()
+    pool.close()
+
+
+def test_pool_cuda_graph_and_rows_growing_past_the_budget():
+    # inserts grow rows after a reload; the pool compacts and evicts to fit
+    graphs, colors, seqs = make_workload(6, seed=8, rounds=3)
+    want = oracle_runs(graphs, colors, seqs, po.HI)
+    nmax = max(n for n, _, _ in graphs)
+    slots = int(2.5 * max(2 * len(a) for _, a, _ in graphs) * 1.25) + 32 * nmax
+    pool = ResidentPool(vertex_capacity=2 * nmax + 16, pool_slots=slots, max_graphs=8, cuda_graph=True)
+    for (n, a, b), c in zip(graphs, colors):
+        pool.add_graph(n, a, b, c)
+    its = [[] for _ in graphs]
+    for r in range(3):
+        for g in range(len(graphs)):
+            st, it, _ = pool.apply([(g, seqs[g][r])])
+            its[g].append(int(it[0]))
+    for g, (cw, iw) in enumerate(want):
+        assert np.array_equal(pool.colors(g), cw)
+        assert its[g] == iw
+    pool.close()
