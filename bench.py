@@ -56,9 +56,18 @@ def parse_args():
                     help="change lines of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-iter-cap", type=int, default=400)
-    ap.add_argument("--mode", choices=["plain", "batched"], default="plain",
-                    help="plain: one large graph (headline); batched: many graphs in one launch")
+    ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
+                    help="plain: one large graph (headline); batched: many graphs in one launch; "
+                         "served: request stream over resident graphs")
     ap.add_argument("--graphs", type=int, default=4096, help="batched mode: number of graphs")
+    ap.add_argument("--served-graphs", type=int, default=256, help="served mode: resident graphs")
+    ap.add_argument("--served-smin", type=int, default=14, help="served mode: smallest graph scale")
+    ap.add_argument("--served-smax", type=int, default=20, help="served mode: largest graph scale")
+    ap.add_argument("--requests", type=int, default=1000, help="served mode: requests per run")
+    ap.add_argument("--loads", default="1000,10000,50000", help="served mode: offered loads, requests/s")
+    ap.add_argument("--budget-frac", type=float, default=0.5,
+                    help="served mode: device row and vertex budget as a fraction of the total graph state")
+    ap.add_argument("--max-lines", type=int, default=1 << 22, help="served mode: lines per shared launch")
     return ap.parse_args()
 
 
@@ -559,10 +568,152 @@ def run_batched(args):
     }
 
 
+# ---------------------------------------------------------------------------
+# served mode: a request stream over resident graphs
+# ---------------------------------------------------------------------------
+
+def build_served_workload(args):
+    """Graphs: two of every three from the R-MAT generator of the single-graph
+    workloads (a=0.57, b=c=0.19, edgefactor 16), the third from the skewed
+    Chung-Lu generator (exponent 2.1, average degree 24, maximum degree n/20),
+    each with 2^s vertices, s uniform in [smin, smax], greedy initial colours.
+    Requests: Poisson arrivals (unit rate here, scaled per offered load),
+    targets Zipf(1.1), sizes log-uniform in [10, 1M] lines; each graph's
+    requests are drawn in order from its evolving edge set with the batch
+    rule of its generator's workload (R-MAT: half deletions, R-MAT endpoints;
+    Chung-Lu: 30% deletions, one inserted endpoint by degree)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import dyncolor_b200 as dc
+    from dyncolor_b200.serve import make_trace
+
+    G = args.served_graphs
+    rng = np.random.default_rng(args.seed + 17)
+    scales = rng.integers(args.served_smin, args.served_smax + 1, G)
+    arrivals, targets, sizes = make_trace(args.requests, G, 1.0, args.seed)
+    mine = [[] for _ in range(G)]
+    for j, g in enumerate(targets):
+        mine[int(g)].append(j)
+
+    def one(i):
+        s = int(scales[i])
+        n = 1 << s
+        seed = args.seed * 1_000_003 + i
+        if i % 3 == 2:
+            a, b = dc.chung_lu(n, 2.1, 24.0, n / 20.0, seed=seed)
+        else:
+            a, b = dc.rmat(s, 16 * n, seed=seed)
+        a, b = dc.dedup(n, a, b)
+        c = dc.greedy_color(n, a, b)
+        lines = {}
+        if mine[i]:
+            es = dc.EdgeSet(n, a, b)
+            alive = len(a)  # deletions are drawn from the original edges still present
+            for r, j in enumerate(mine[i]):
+                k = int(sizes[j])
+                if i % 3 == 2:
+                    kd = min(int(0.3 * k), alive)
+                    x = es.sample_batch(kd, k - kd, mode=dc.INS_DEGREE, seed=seed * 31 + r)
+                else:
+                    kd = min(k // 2, alive)
+                    x = es.sample_batch(kd, k - kd, mode=dc.INS_RMAT, scale=s, seed=seed * 31 + r)
+                alive -= kd
+                lines[j] = x
+        return (n, a, b), c, lines
+
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        out = list(ex.map(one, range(G)))
+    graphs = [o[0] for o in out]
+    colors = [o[1] for o in out]
+    req_lines = [None] * len(targets)
+    for o in out:
+        for j, x in o[2].items():
+            req_lines[j] = x
+    return graphs, colors, arrivals, targets, req_lines, scales
+
+
+def run_served(args):
+    import dyncolor_b200 as dc
+    from dyncolor_b200.pool import ResidentPool
+    from dyncolor_b200.serve import Request, Server
+
+    variant = dc.HI if args.variant == "hi" else dc.HB
+    t0 = time.time()
+    graphs, colors, arrivals, targets, req_lines, scales = build_served_workload(args)
+    gen_s = time.time() - t0
+    nsum = sum(n for n, _, _ in graphs)
+    nmax = max(n for n, _, _ in graphs)
+    est_slots = sum(int(2.5 * len(a)) + 4 * n for n, a, _ in graphs)
+    state_bytes = 4 * est_slots + 36 * nsum
+    vcap = max(int(args.budget_frac * nsum), 2 * nmax)
+    slots = max(int(args.budget_frac * est_slots), 4 * max(int(2.5 * len(a)) + 4 * n for n, a, _ in graphs))
+    lines_total = int(sum(len(x) for x in req_lines))
+    loads = [float(x) for x in args.loads.split(",") if x]
+    runs, first_colors, first_its, exact = [], None, None, True
+    for rate in loads:
+        for policy in ("plain", "batched"):
+            pool = ResidentPool(variant=variant, vertex_capacity=vcap, pool_slots=slots,
+                                pool_slots_max=4 * slots, max_graphs=len(graphs) + 1, cuda_graph=True)
+            tb = time.time()
+            for (n, a, b), c in zip(graphs, colors):
+                pool.add_graph(n, a, b, c)
+            build_s = time.time() - tb
+            info0 = pool.info()
+            reqs = [Request(j, int(targets[j]), req_lines[j], float(arrivals[j]) / rate)
+                    for j in range(len(targets))]
+            st = Server(pool, policy, vcap, slots, max_lines=args.max_lines).run(reqs)
+            info1 = pool.info()
+            fin = [pool.colors(g) for g in range(len(graphs))]
+            its = np.array([r.iterations for r in sorted(reqs, key=lambda r: r.rid)])
+            if first_colors is None:
+                first_colors, first_its = fin, its
+            else:
+                exact = exact and all(np.array_equal(x, y) for x, y in zip(fin, first_colors)) \
+                    and bool(np.array_equal(its, first_its))
+            summ = st.summary(reqs)
+            summ.update({
+                "offered_req_per_s": rate, "policy": policy, "pool_build_s": round(build_s, 2),
+                "restores": info1["restores"] - info0["restores"], "spills": info1["spills"] - info0["spills"],
+                "restore_ms": round(info1["restore_ms"] - info0["restore_ms"], 1),
+                "spill_ms": round(info1["spill_ms"] - info0["spill_ms"], 1),
+                "compactions": info1["compactions"] - info0["compactions"],
+                "device_gb": round(info1["device_bytes"] / 1e9, 2),
+                "pinned_host_gb": round(info1["host_bytes"] / 1e9, 2),
+            })
+            runs.append(summ)
+            pool.close()
+    top = [r for r in runs if r["offered_req_per_s"] == max(loads)]
+    best = next(r for r in top if r["policy"] == "batched")
+    plain = next(r for r in top if r["policy"] == "plain")
+    return {
+        "metric": METRIC, "value": best["updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(runs),
+        "warmup": 0, "ms_per_step": best["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic", "mode": "served",
+        "config": {"workload": (f"{len(graphs)} resident graphs (R-MAT ef16 and Chung-Lu 2.1, 2^s vertices, "
+                                f"s in [{args.served_smin}, {args.served_smax}]), {len(targets)} requests, "
+                                f"Poisson arrivals, Zipf(1.1) targets, log-uniform [10, 1M] lines, variant "
+                                f"{args.variant.upper()}"),
+                   "vertices": nsum, "edges": int(sum(len(a) for _, a, _ in graphs)), "lines": lines_total,
+                   "graph_state_gb": round(state_bytes / 1e9, 2), "budget_frac": args.budget_frac,
+                   "vertex_capacity": vcap, "pool_slots": slots, "max_lines_per_launch": args.max_lines},
+        "e2e": {"value": best["updates_per_s"], "unit": UNIT,
+                "h2d_bytes_per_step": 12 * lines_total, "d2h_bytes_per_step": 0},
+        "plain_one_batch_per_launch": {"value": plain["updates_per_s"], "p50_ms": plain["p50_ms"],
+                                       "p99_ms": plain["p99_ms"]},
+        "speedup_vs_plain": best["updates_per_s"] / plain["updates_per_s"] if plain["updates_per_s"] else None,
+        "bit_exact_across_policies": exact,
+        "runs": runs,
+        "detail": {"workload_gen_s": round(gen_s, 1), "scales": np.bincount(scales).tolist()},
+    }
+
+
 def main():
     args = parse_args()
     if args.mode == "batched":
         print(json.dumps(run_batched(args)), flush=True)
+        return
+    if args.mode == "served":
+        print(json.dumps(run_served(args)), flush=True)
         return
     if args.impl == "reference":
         # the reference has no GPU path here: rank 0 times it, other ranks exit

@@ -241,46 +241,77 @@ dc_status read_state(dc_ctx* ctx) {
 void drop_graph(dc_ctx* ctx);
 
 // Moves the adjacency into a fresh pool of new_cap slots (tombstones dropped).
+// Packed size of every row (tombstones dropped, rows at the repack slack).
+dc_status packed_total(dc_ctx* ctx, long long* total, long long** scratch_out) {
+  const long long n = std::max(ctx->n, 1);
+  long long* scratch = nullptr;
+  dc_status s;
+  if ((s = dalloc(ctx, &scratch, n / 256 + 2, "repack scratch")) != DC_OK) return s;
+  cudaError_t e = launch_packed_total(graph_dev(ctx), ctx->opt.slack, scratch, ctx->d_scalar, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->h_scalar, ctx->d_scalar, 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    dfree(ctx, &scratch);
+    return cuda_fail(ctx, "packed total", e);
+  }
+  *total = (long long)ctx->h_scalar[0];
+  if (scratch_out)
+    *scratch_out = scratch;
+  else
+    dfree(ctx, &scratch);
+  return DC_OK;
+}
+
+// Moves the adjacency into a fresh pool of new_cap slots (tombstones
+// dropped).  Nothing changes when the packed rows need more than new_cap.
 dc_status repack(dc_ctx* ctx, long long new_cap) {
-  GraphDev g = graph_dev(ctx);
+  long long total = 0;
+  long long* scratch = nullptr;
+  dc_status s;
+  if ((s = packed_total(ctx, &total, &scratch)) != DC_OK) return s;
+  if (total > new_cap) {
+    dfree(ctx, &scratch);
+    return fail(ctx, DC_E_NOMEM, "compaction needs " + std::to_string(total) + " adjacency slots, the pool has " +
+                                     std::to_string(new_cap));
+  }
   long long* off2 = nullptr;
   int* cap2 = nullptr;
+  int* len2 = nullptr;
   int* adj2 = nullptr;
-  long long* scratch = nullptr;
   const long long n = std::max(ctx->n, 1);
-  dc_status s;
-  if ((s = dalloc(ctx, &off2, n, "repack offsets")) != DC_OK) return s;
-  if ((s = dalloc(ctx, &cap2, n, "repack caps")) != DC_OK) {
-    dfree(ctx, &off2);
-    return s;
-  }
-  if ((s = dalloc(ctx, &adj2, new_cap, "repack pool")) != DC_OK) {
+  auto drop = [&]() {
+    dfree(ctx, &scratch);
     dfree(ctx, &off2);
     dfree(ctx, &cap2);
-    return s;
-  }
-  if ((s = dalloc(ctx, &scratch, n / 256 + 2, "repack scratch")) != DC_OK) {
-    dfree(ctx, &off2);
-    dfree(ctx, &cap2);
+    dfree(ctx, &len2);
     dfree(ctx, &adj2);
+  };
+  if ((s = dalloc(ctx, &off2, n, "repack offsets")) != DC_OK || (s = dalloc(ctx, &cap2, n, "repack caps")) != DC_OK ||
+      (s = dalloc(ctx, &len2, n, "repack lengths")) != DC_OK ||
+      (s = dalloc(ctx, &adj2, new_cap, "repack pool")) != DC_OK) {
+    drop();
     return s;
   }
   DC_CK(cudaMemsetAsync(&ctx->st->status, 0, sizeof(unsigned), ctx->stream));
-  DC_CK(launch_repack(g, off2, cap2, adj2, new_cap, ctx->opt.slack, &ctx->st->pool_used, &ctx->st->status,
-                      scratch, ctx->stream));
+  DC_CK(launch_repack_copy(graph_dev(ctx), ctx->opt.slack, scratch, off2, cap2, len2, adj2, new_cap,
+                           &ctx->st->status, ctx->stream));
   if ((s = read_state(ctx)) != DC_OK) return s;
-  dfree(ctx, &scratch);
-  if ((ctx->h_st->status & ST_OVERFLOW) || (long long)ctx->h_st->pool_used > new_cap) {
-    dfree(ctx, &off2);
-    dfree(ctx, &cap2);
-    dfree(ctx, &adj2);
-    return fail(ctx, DC_E_INTERNAL, "repack: pool too small");
+  if (ctx->h_st->status & ST_OVERFLOW) {
+    drop();
+    return fail(ctx, DC_E_INTERNAL, "repack: a row outgrew its packed size");
   }
+  ctx->h_scalar[1] = (unsigned long long)total;
+  DC_CK(cudaMemcpyAsync(&ctx->st->pool_used, ctx->h_scalar + 1, 8, cudaMemcpyHostToDevice, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  dfree(ctx, &scratch);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->cap);
+  dfree(ctx, &ctx->len);
   dfree(ctx, &ctx->adj);
   ctx->off = off2;
   ctx->cap = cap2;
+  ctx->len = len2;
   ctx->adj = adj2;
   ctx->pool_cap = new_cap;
   drop_graph(ctx);  // a captured batch graph names the old arrays

@@ -161,6 +161,7 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx);
 dc_status reset_bitmaps(dc_ctx* ctx);
 dc_status read_state(dc_ctx* ctx);
 dc_status repack(dc_ctx* ctx, long long new_cap);
+dc_status packed_total(dc_ctx* ctx, long long* total, long long** scratch_out);
 dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int* lb, long long k, bool recolor,
                     dc_stats* out);
 bool ready(dc_ctx* ctx);

@@ -178,10 +178,13 @@ cudaError_t launch_color_unmark(const GraphDev& g, cudaStream_t s);
 // Batched mode: gid[v] from graph start offsets; counts edges crossing graphs.
 cudaError_t launch_partition(const GraphDev& g, const int* first, int ngraphs, int* gid,
                              unsigned long long* cross, cudaStream_t s);
-// Repacks rows of g into new arrays (off2/cap2/adj2) with the given slack.
-cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* adj2,
-                          long long cap_slots, float slack, unsigned long long* used,
-                          unsigned* status, long long* scratch, cudaStream_t s);
+// Repacking rows of g into new arrays with the given slack, in two parts:
+// the packed total (scratch: ceil(n / 256) + 1 long longs), then the copy
+// into off2/cap2/len2/adj2 (g itself is only read).
+cudaError_t launch_packed_total(const GraphDev& g, float slack, long long* scratch, unsigned long long* total,
+                                cudaStream_t s);
+cudaError_t launch_repack_copy(const GraphDev& g, float slack, const long long* scratch, long long* off2, int* cap2,
+                               int* len2, int* adj2, long long cap_slots, unsigned* status, cudaStream_t s);
 // Resident pool: copy the rows of vertices [v0, v0 + nv) out to / in from a
 // packed buffer (row i at pre[i]), with vertex ids shifted by -base / +base.
 cudaError_t launch_range_gather(const GraphDev& g, int base, int v0, int nv, const long long* pre, int* out,

@@ -150,8 +150,9 @@ __global__ void repack_offsets_kernel(GraphDev g, float slack, const long long* 
   }
 }
 
-// repack step 4: order-preserving copy of the live slots, one warp per row
-__global__ void repack_copy_kernel(GraphDev g, const long long* off2, int* adj2, long long cap_slots,
+// repack step 4: order-preserving copy of the live slots, one warp per row;
+// the new row lengths go to len2 so the old layout stays whole until the swap
+__global__ void repack_copy_kernel(GraphDev g, const long long* off2, int* len2, int* adj2, long long cap_slots,
                                    unsigned* status) {
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -174,7 +175,7 @@ __global__ void repack_copy_kernel(GraphDev g, const long long* off2, int* adj2,
       cur += __popc(bal);
     }
     __syncwarp();
-    if (lane_id() == 0) g.len[v] = cur;
+    if (lane_id() == 0) len2[v] = cur;
   }
 }
 
@@ -266,17 +267,25 @@ cudaError_t launch_partition(const GraphDev& g, const int* first, int ngraphs, i
   return cudaGetLastError();
 }
 
-// scratch must hold ceil(n / 256) + 1 long longs.
-cudaError_t launch_repack(const GraphDev& g, long long* off2, int* cap2, int* adj2, long long cap_slots,
-                          float slack, unsigned long long* used, unsigned* status, long long* scratch,
-                          cudaStream_t s) {
+// scratch must hold ceil(n / 256) + 1 long longs.  Steps 1-2: per-block
+// offsets in scratch and the packed total in *total.
+cudaError_t launch_packed_total(const GraphDev& g, float slack, long long* scratch, unsigned long long* total,
+                                cudaStream_t s) {
   const long long nb = ((long long)g.n + kMiscThreads - 1) / kMiscThreads;
-  if (nb == 0) return cudaMemsetAsync(used, 0, sizeof(unsigned long long), s);
+  if (nb == 0) return cudaMemsetAsync(total, 0, sizeof(unsigned long long), s);
   repack_caps_kernel<<<(unsigned)nb, kMiscThreads, 0, s>>>(g, slack, scratch);
-  repack_scan_kernel<<<1, kMiscThreads, 0, s>>>(scratch, nb, used);
+  repack_scan_kernel<<<1, kMiscThreads, 0, s>>>(scratch, nb, total);
+  return cudaGetLastError();
+}
+
+// Steps 3-4 with the scratch of launch_packed_total.
+cudaError_t launch_repack_copy(const GraphDev& g, float slack, const long long* scratch, long long* off2, int* cap2,
+                               int* len2, int* adj2, long long cap_slots, unsigned* status, cudaStream_t s) {
+  const long long nb = ((long long)g.n + kMiscThreads - 1) / kMiscThreads;
+  if (nb == 0) return cudaSuccess;
   repack_offsets_kernel<<<(unsigned)nb, kMiscThreads, 0, s>>>(g, slack, scratch, off2, cap2);
   repack_copy_kernel<<<misc_grid((long long)g.n * 32, kMiscThreads), kMiscThreads, 0, s>>>(
-      g, off2, adj2, cap_slots, status);
+      g, off2, len2, adj2, cap_slots, status);
   return cudaGetLastError();
 }
 

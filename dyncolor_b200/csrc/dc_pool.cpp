@@ -81,6 +81,8 @@ struct dc_pool {
   int* h_giters = nullptr;        // pinned, G + 1
   std::unordered_map<void*, long long> hsizes;
   long long host_bytes = 0;
+  long long budget = 0;  // adjacency slots for the packed rows of resident graphs
+  long long hard = 0;    // the pool never grows past this
   dc_pool_info info{};
 };
 
@@ -190,10 +192,21 @@ dc_status read_used(dc_pool* P, long long* used) {
   return DC_OK;
 }
 
-dc_status compact(dc_pool* P) {
+// Compacts the pool to max(budget, packed rows + extra) slots: back to the
+// budget when the resident rows allow it, past it (up to the hard limit)
+// when the graphs that must stay resident need more.
+dc_status compact(dc_pool* P, long long extra) {
   dc_ctx* ctx = P->u;
-  dc_status s = repack(ctx, ctx->pool_cap);
+  long long T = 0;
+  dc_status s = packed_total(ctx, &T, nullptr);
   if (s != DC_OK) return s;
+  const long long target = (std::max(P->budget, T + extra) + 3) & ~3ll;
+  if (target > P->hard)
+    return pfail(P, DC_E_NOMEM, "resident rows need " + std::to_string(T + extra) +
+                                    " adjacency slots, past the pool's hard limit of " + std::to_string(P->hard));
+  if ((s = repack(ctx, target)) != DC_OK) return s;
+  ctx->max_pool_cap = target;  // growth inside a launch stops here
+  if (target > P->budget) ++P->info.overbudget;
   ++P->info.compactions;
   DC_CK(cudaStreamSynchronize(ctx->stream));
   return DC_OK;
@@ -298,41 +311,59 @@ dc_status spill(dc_pool* P, int gi) {
 }
 
 // Finds vertex ids [start, start + n) and `need` free slots at the pool's
-// tail, evicting least recently used unlocked graphs and compacting the
-// pool as needed.  *base = pool_used afterwards (the tail's start).
+// tail: evicts least recently used unlocked graphs until the packed rows of
+// the resident graphs plus `need` fit the budget (or nothing is left to
+// evict), then compacts when the tail is short.  *base = the tail's start.
 dc_status make_room(dc_pool* P, int n, long long need, const std::vector<char>& locked, int* start,
                     long long* base) {
   dc_ctx* ctx = P->u;
   dc_status s;
-  if (need > ctx->pool_cap)
-    return pfail(P, DC_E_NOMEM, "a graph needs " + std::to_string(need) + " adjacency slots; the pool has " +
-                                    std::to_string(ctx->pool_cap));
+  if (need > P->hard)
+    return pfail(P, DC_E_NOMEM, "a graph needs " + std::to_string(need) + " adjacency slots; the pool's hard limit is " +
+                                    std::to_string(P->hard));
   while (!find_range(P, n, start)) {
     const int v = lru_victim(P, locked);
     if (v < 0) return pfail(P, DC_E_NOMEM, "vertex capacity exhausted by graphs this launch needs");
     if ((s = spill(P, v)) != DC_OK) return s;
   }
+  long long T = 0;
+  if ((s = packed_total(ctx, &T, nullptr)) != DC_OK) return s;
+  while (T + need > P->budget) {
+    const int v = lru_victim(P, locked);
+    if (v < 0) break;  // the locked graphs alone exceed the budget
+    if ((s = spill(P, v)) != DC_OK) return s;
+    T -= P->graphs[(size_t)v].packed;
+  }
   long long used = 0;
   if ((s = read_used(P, &used)) != DC_OK) return s;
-  if (used + need > ctx->pool_cap) {
-    if ((s = compact(P)) != DC_OK) return s;
+  if (used + need > ctx->pool_cap || (ctx->pool_cap > P->budget && T + need <= P->budget)) {
+    if ((s = compact(P, need)) != DC_OK) return s;
     if ((s = read_used(P, &used)) != DC_OK) return s;
-    long long est = used;
-    bool evicted = false;
-    while (est + need > ctx->pool_cap) {
-      const int v = lru_victim(P, locked);
-      if (v < 0) return pfail(P, DC_E_NOMEM, "adjacency budget exhausted by graphs this launch needs");
-      if ((s = spill(P, v)) != DC_OK) return s;
-      est -= P->graphs[(size_t)v].packed;
-      evicted = true;
-    }
-    if (evicted) {
-      if ((s = compact(P)) != DC_OK) return s;
-      if ((s = read_used(P, &used)) != DC_OK) return s;
-    }
-    if (used + need > ctx->pool_cap) return pfail(P, DC_E_NOMEM, "adjacency budget exhausted after compaction");
   }
+  if (used + need > ctx->pool_cap) return pfail(P, DC_E_NOMEM, "adjacency pool short after compaction");
   *base = used;
+  return DC_OK;
+}
+
+// After a launch found the pool short (an exhausted launch changes
+// nothing): evicts the least recently used unlocked graph, or, with none
+// left, grows the pool past the budget toward the hard limit.
+dc_status relieve(dc_pool* P, const std::vector<char>& locked, long long lines) {
+  dc_ctx* ctx = P->u;
+  const int v = lru_victim(P, locked);
+  dc_status s;
+  if (v >= 0) {
+    if ((s = spill(P, v)) != DC_OK) return s;
+    return compact(P, 0);
+  }
+  if (ctx->pool_cap >= P->hard)
+    return pfail(P, DC_E_NOMEM, "the graphs of this launch outgrew the pool's hard limit");
+  const long long target =
+      std::min(P->hard, ctx->pool_cap + std::max(ctx->pool_cap / 2, 4 * lines + 4096)) & ~3ll;
+  if ((s = repack(ctx, target)) != DC_OK) return s;
+  ctx->max_pool_cap = target;
+  ++P->info.overbudget;
+  ++P->info.compactions;
   return DC_OK;
 }
 
@@ -458,7 +489,9 @@ dc_status dc_pool_create(dc_pool** out, const dc_pool_options* opt) {
     dc_pool_destroy(P);
     return st;
   };
-  ctx->max_pool_cap = (o.pool_slots + 3) & ~3ll;
+  P->budget = (o.pool_slots + 3) & ~3ll;
+  P->hard = std::max(P->budget, (o.pool_slots_max > 0 ? o.pool_slots_max : 2 * o.pool_slots) & ~3ll);
+  ctx->max_pool_cap = P->budget;
   if ((s = dc_graph_load_edges(ctx, o.vertex_capacity, nullptr, nullptr, 0)) != DC_OK) return bail(s);
   P->G = o.max_graphs;
   const long long G1 = (long long)P->G + 1;
@@ -541,7 +574,7 @@ dc_status dc_pool_add_graph(dc_pool* P, int32_t n, const int32_t* a, const int32
   int f = 0;
   long long base = 0;
   dc_status s;
-  if ((s = make_room(P, n, std::min(need, ctx->pool_cap), locked, &f, &base)) != DC_OK) return undo(s);
+  if ((s = make_room(P, n, std::min(need, P->budget), locked, &f, &base)) != DC_OK) return undo(s);
   take_range(P, f, n);
   PGraph& g = P->graphs[(size_t)gi];
   g.resident = true;
@@ -573,12 +606,8 @@ dc_status dc_pool_add_graph(dc_pool* P, int32_t n, const int32_t* a, const int32
       for (;;) {
         s = run_batch(ctx, nullptr, da, db, len, false, nullptr);
         if (s != DC_E_NOMEM) break;
-        // the pool ran short of the estimate: evict another graph and retry
-        // (an exhausted launch modifies nothing)
-        const int v = lru_victim(P, locked);
-        if (v < 0) break;
-        if ((s = spill(P, v)) != DC_OK) break;
-        if ((s = compact(P)) != DC_OK) break;
+        // the rows outgrew the estimate: make room and retry
+        if ((s = relieve(P, locked, len)) != DC_OK) break;
       }
     }
     dfree(ctx, &da);
@@ -632,7 +661,7 @@ dc_status dc_pool_apply(dc_pool* P, const dc_pool_request* reqs, int32_t count, 
     nsum += n;
     slots += P->graphs[(size_t)r.graph].packed;
   }
-  if (nsum > P->opt.vertex_capacity || slots > ctx->pool_cap)
+  if (nsum > P->opt.vertex_capacity || slots > P->hard)
     return pfail(P, DC_E_NOMEM, "the graphs of this launch do not fit the pool together");
   if (K > (1ll << 30)) return pfail(P, DC_E_INVAL, "more than 2^30 change lines in one launch");
   cudaSetDevice(ctx->device);
@@ -668,13 +697,9 @@ dc_status dc_pool_apply(dc_pool* P, const dc_pool_request* reqs, int32_t count, 
     for (;;) {
       s = dc_apply_batch(ctx, P->h_lines, K, stats);
       if (s != DC_E_NOMEM) break;
-      // rows grew past the budget: evict an idle graph and retry (the
-      // exhausted launch modified nothing)
-      const int v = lru_victim(P, locked);
-      if (v < 0) break;
-      dc_status s2;
-      if ((s2 = spill(P, v)) != DC_OK) return s2;
-      if ((s2 = compact(P)) != DC_OK) return s2;
+      // rows grew past the pool: make room and retry
+      dc_status s2 = relieve(P, locked, K);
+      if (s2 != DC_OK) return s2;
     }
     if (s != DC_OK && s != DC_E_ITER_LIMIT) return s;
     DC_CK(cudaMemcpyAsync(P->h_giters, ctx->giters, (size_t)(P->G + 1) * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -744,6 +769,8 @@ dc_status dc_pool_info_get(dc_pool* P, dc_pool_info* info) {
   info->vertex_capacity = P->opt.vertex_capacity;
   info->pool_slots_used = used;
   info->pool_slots = P->u->pool_cap;
+  info->pool_slots_budget = P->budget;
+  info->pool_slots_max = P->hard;
   info->device_bytes = P->u->bytes;
   info->host_bytes = P->host_bytes;
   return DC_OK;

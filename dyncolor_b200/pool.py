@@ -30,6 +30,7 @@ class PoolOptions(C.Structure):
         ("unit_slots", C.c_int32),
         ("cuda_graph", C.c_int32),
         ("stage_slots", C.c_int64),
+        ("pool_slots_max", C.c_int64),
         ("reserved", C.c_int32 * 8),
     ]
 
@@ -50,6 +51,9 @@ class PoolInfo(C.Structure):
         ("vertex_capacity", C.c_int64),
         ("pool_slots_used", C.c_int64),
         ("pool_slots", C.c_int64),
+        ("pool_slots_budget", C.c_int64),
+        ("pool_slots_max", C.c_int64),
+        ("overbudget", C.c_int64),
         ("spills", C.c_int64),
         ("restores", C.c_int64),
         ("spill_bytes", C.c_int64),
@@ -99,7 +103,7 @@ class ResidentPool:
     def __init__(self, variant: int = HI, vertex_capacity: int = 1 << 22, pool_slots: int = 1 << 28,
                  max_graphs: int = 1024, device: int = 0, iter_cap: int = 0, slack: float = 0.0,
                  blocks_per_sm: int = 0, unit_slots: int = 0, cuda_graph: bool = False,
-                 stage_slots: int = 0, stream: int = 0):
+                 stage_slots: int = 0, pool_slots_max: int = 0, stream: int = 0):
         L = _lib()
         o = PoolOptions()
         L.dc_pool_options_default(C.byref(o))
@@ -119,6 +123,7 @@ class ResidentPool:
         o.cuda_graph = 1 if cuda_graph else 0
         if stage_slots:
             o.stage_slots = stage_slots
+        o.pool_slots_max = pool_slots_max
         h = C.c_void_p()
         rc = L.dc_pool_create(C.byref(h), C.byref(o))
         if rc != OK:

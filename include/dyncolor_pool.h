@@ -14,8 +14,11 @@
  *  - Admission is by budget.  A graph that is not resident is held in pinned
  *    host memory (its rows, colours, previous colours and degree property);
  *    bringing it back evicts the least recently used graphs that the current
- *    launch does not touch, and compacts the adjacency pool when its free
- *    tail is too short.  Spill and reload are exact copies.
+ *    launch does not touch until the packed rows of the resident graphs fit
+ *    pool_slots, and compacts the adjacency pool when its free tail is too
+ *    short.  Spill and reload are exact copies.  Only when the graphs of one
+ *    launch alone need more than pool_slots does the pool grow past it, up
+ *    to pool_slots_max; otherwise the call fails with DC_E_NOMEM.
  *  - Lines use each graph's own vertex ids [0, n).  Lines with an inst other
  *    than 0 or 1 are ignored, as readin_changes ignores them.
  *
@@ -44,6 +47,9 @@ typedef struct {
   int32_t unit_slots;      /* adjacency slots per warp work unit; 0: 2048 */
   int32_t cuda_graph;      /* 1: replay each launch from a captured CUDA graph */
   int64_t stage_slots;     /* device staging for spill and reload (4-byte slots); <= 0: 2^25 */
+  int64_t pool_slots_max;  /* hard limit: when the graphs of one launch alone outgrow pool_slots, the
+                              pool grows up to this many slots (and shrinks back at the next
+                              compaction that allows it); <= 0: 2 * pool_slots */
   int32_t reserved[8];
 } dc_pool_options;
 
@@ -67,7 +73,10 @@ typedef struct {
   int64_t resident_vertices;
   int64_t vertex_capacity;
   int64_t pool_slots_used; /* adjacency pool slots handed out (live rows and garbage) */
-  int64_t pool_slots;
+  int64_t pool_slots;      /* current adjacency pool size */
+  int64_t pool_slots_budget;
+  int64_t pool_slots_max;
+  int64_t overbudget;      /* compactions or launches that took the pool past its budget */
   int64_t spills;
   int64_t restores;
   int64_t spill_bytes;     /* device -> host bytes moved by spills */

@@ -137,3 +137,46 @@ def test_pool_cuda_graph_and_rows_growing_past_the_budget():
         assert np.array_equal(pool.colors(g), cw)
         assert its[g] == iw
     pool.close()
+
+
+def test_pool_grows_past_budget_only_for_one_launch_and_shrinks_back():
+    # one graph whose batch triples its edges cannot fit the budget: the pool
+    # grows up to its hard limit for that launch, then returns to the budget
+    n = 2000
+    a, b = dc.uniform_pairs(n, 4000, seed=5)
+    a, b = dc.dedup(n, a, b)
+    col = dc.greedy_color(n, a, b)
+    es = dc.EdgeSet(n, a, b)
+    big = es.sample_batch(100, 12000, seed=9)
+    small_n = 500
+    sa, sb = dc.uniform_pairs(small_n, 1000, seed=6)
+    sa, sb = dc.dedup(small_n, sa, sb)
+    scol = dc.greedy_color(small_n, sa, sb)
+    budget = int(2.5 * len(a)) + 8 * n + int(2.5 * len(sa)) + 8 * small_n
+    o = oracle_graph(n, a, b, col)
+    rc, so = o.apply_batch(to_oracle_changes(big), po.HI, po.SNAPSHOT)
+    assert rc == po.OK
+    # a hard limit equal to the budget: the launch fails and changes nothing
+    tight = ResidentPool(vertex_capacity=4 * n, pool_slots=budget, pool_slots_max=budget, max_graphs=4)
+    g0 = tight.add_graph(n, a, b, col)
+    with pytest.raises(dc.DcError) as e:
+        tight.apply([(g0, big)])
+    assert e.value.status == dc.E_NOMEM
+    assert np.array_equal(tight.colors(g0), col)
+    tight.close()
+    pool = ResidentPool(vertex_capacity=4 * n, pool_slots=budget, pool_slots_max=8 * budget, max_graphs=4)
+    g0 = pool.add_graph(n, a, b, col)
+    g1 = pool.add_graph(small_n, sa, sb, scol)
+    st, it, _ = pool.apply([(g0, big)])
+    assert np.array_equal(pool.colors(g0), o.colors()) and it[0] == so.iterations
+    info = pool.info()
+    assert info["overbudget"] > 0 and info["pool_slots"] > info["pool_slots_budget"]
+    assert not pool.graph_size(g1)[2]  # evicted before the pool grew
+    # the big graph spilled: the small one comes back and the pool shrinks to its budget
+    pool.spill(g0)
+    st, it, _ = pool.apply([(g1, np.empty(0, dtype=dc.CHANGE_DTYPE))])
+    info = pool.info()
+    assert info["pool_slots"] == info["pool_slots_budget"]
+    assert np.array_equal(pool.colors(g1), scol)
+    assert np.array_equal(pool.colors(g0), o.colors())
+    pool.close()
