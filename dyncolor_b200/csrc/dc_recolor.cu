@@ -235,14 +235,23 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
   // load is coalesced across the warp, and because rows are kept sorted by
   // neighbour id, the colour gathers of one instruction fall on nearby
   // addresses in dense rows.  Four independent gathers are in flight.
+  // The ids of round r + 1 are loaded before the colour gathers of round r
+  // are consumed, so each round waits on one dependent load, not two.
+  int nx[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int sidx = s_lo + j * 32 + lane_id();
+    nx[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
+  }
   for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
     int uu[4];
     bool ok[4];
     int cc[4], pp[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int sidx = r0 + j * 32 + lane_id();
-      uu[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
+      uu[j] = nx[j];
+      const int sidx = r0 + 128 + j * 32 + lane_id();
+      nx[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) ok[j] = uu[j] >= 0;
@@ -436,14 +445,21 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
   R.cv = g.color[v] & kColorMask;
   R.pv = E.variant == DC_HI ? g.prev[v] : g.prop[v];
   bool markv = false;
+  int nx[4];  // ids of the next round, loaded one round ahead
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int sidx = s_lo + j * 32 + lane_id();
+    nx[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
+  }
   for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
     int uu[4], cc[4], pp[4];
     unsigned ww[4];
     bool mu[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-      const int sidx = r0 + j * 32 + lane_id();
-      uu[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
+      uu[j] = nx[j];
+      const int sidx = r0 + 128 + j * 32 + lane_id();
+      nx[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
     }
     // one gather gives u's colour and its next-frontier mark
 #pragma unroll
