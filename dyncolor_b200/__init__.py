@@ -113,6 +113,7 @@ def lib() -> C.CDLL:
     L.dc_destroy.restype = None
     L.dc_graph_load_edges.argtypes = [P, C.c_int32, P, P, C.c_int64]
     L.dc_colors_set.argtypes = [P, P, C.c_int32]
+    L.dc_colors_init_greedy.argtypes = [P]
     L.dc_apply_batch.argtypes = [P, P, C.c_int64, C.POINTER(Stats)]
     L.dc_apply_batch_device.argtypes = [P, P, C.c_int64, C.POINTER(Stats)]
     L.dc_colors_read.argtypes = [P, P, C.c_int32]
@@ -230,6 +231,10 @@ class Context:
     def set_colors(self, colors):
         c = np.ascontiguousarray(colors, dtype=np.int32)
         self._check(lib().dc_colors_set(self._h, _ptr(c), len(c)), "dc_colors_set")
+
+    def init_greedy_colors(self):
+        """Greedy lowest-free colouring in vertex-id order of the current graph."""
+        self._check(lib().dc_colors_init_greedy(self._h), "dc_colors_init_greedy")
 
     def apply_batch(self, changes, check: bool = True) -> Stats:
         ch = np.ascontiguousarray(changes, dtype=CHANGE_DTYPE)

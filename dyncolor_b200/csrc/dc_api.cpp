@@ -74,6 +74,7 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     if ((s = dalloc(ctx, &ctx->bmC, words, "bitmap")) != DC_OK) return s;
     if ((s = dalloc(ctx, &ctx->ncolor, n, "ncolor")) != DC_OK) return s;
     if ((s = dalloc(ctx, &ctx->sat, n, "sat")) != DC_OK) return s;
+    if (ctx->opt.variant == DC_HB && (s = dalloc(ctx, &ctx->cp, n, "packed words")) != DC_OK) return s;
     DC_CK(cudaMemsetAsync(ctx->bmA, 0, words * 4, ctx->stream));
     DC_CK(cudaMemsetAsync(ctx->bmB, 0, words * 4, ctx->stream));
     DC_CK(cudaMemsetAsync(ctx->bmC, 0, words * 4, ctx->stream));
@@ -210,6 +211,7 @@ RecolorParams recolor_params(dc_ctx* ctx, const dc_change* ch, long long k) {
   p.bmC = ctx->bmC;
   p.ncolor = ctx->ncolor;
   p.sat = ctx->sat;
+  p.cp = ctx->cp;
   p.lflag = ctx->lflag;
   if (ctx->ngraphs > 0) {
     p.gid = ctx->gid;
@@ -590,6 +592,7 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->bmC);
   dfree(ctx, &ctx->ncolor);
   dfree(ctx, &ctx->sat);
+  dfree(ctx, &ctx->cp);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->len);
   dfree(ctx, &ctx->cap);
@@ -692,6 +695,78 @@ dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
   if (n > 0) DC_CK(cudaMemcpyAsync(ctx->color, colors, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  DC_CK(launch_color_max(graph_dev(ctx), ctx->st, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  return DC_OK;
+}
+
+dc_status dc_colors_init_greedy(dc_ctx* ctx) {
+  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  cudaSetDevice(ctx->device);
+  cudaGetLastError();  // start from a clean error state
+  const int n = ctx->n;
+  std::vector<int> live((size_t)std::max(n, 1)), col((size_t)std::max(n, 1), 0);
+  if (n > 0) DC_CK(cudaMemcpyAsync(live.data(), ctx->live, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  DC_CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<long long> pre((size_t)n + 1, 0);
+  int maxlive = 0;
+  for (int v = 0; v < n; ++v) {
+    pre[(size_t)v + 1] = pre[(size_t)v] + live[(size_t)v];
+    maxlive = std::max(maxlive, live[(size_t)v]);
+  }
+  // rows come back in vertex order, a chunk of rows at a time
+  const long long kRows = 1ll << 20;
+  const long long stage_cap = std::max<long long>(1ll << 24, maxlive);
+  long long* dpre = nullptr;
+  int* dstage = nullptr;
+  dc_status s;
+  if ((s = dalloc(ctx, &dpre, kRows + 1, "greedy chunk offsets")) != DC_OK) return s;
+  if ((s = dalloc(ctx, &dstage, stage_cap, "greedy staging")) != DC_OK) {
+    dfree(ctx, &dpre);
+    return s;
+  }
+  std::vector<long long> prerel((size_t)kRows + 1);
+  std::vector<int> rows((size_t)stage_cap);
+  std::vector<unsigned> stamp((size_t)maxlive + 2, 0u);
+  unsigned gen = 0;
+  const GraphDev gd = graph_dev(ctx);
+  cudaError_t e = cudaSuccess;
+  for (int v0 = 0; v0 < n && e == cudaSuccess;) {
+    long long lo = v0 + 1, hi = std::min<long long>(n, (long long)v0 + kRows);
+    while (lo < hi) {  // largest v1 <= hi whose rows fit the stage
+      const long long mid = (lo + hi + 1) / 2;
+      if (pre[(size_t)mid] - pre[(size_t)v0] <= stage_cap) lo = mid; else hi = mid - 1;
+    }
+    const int v1 = (int)lo;
+    for (int i = 0; i <= v1 - v0; ++i) prerel[(size_t)i] = pre[(size_t)v0 + i] - pre[(size_t)v0];
+    const long long cnt = pre[(size_t)v1] - pre[(size_t)v0];
+    e = cudaMemcpyAsync(dpre, prerel.data(), (size_t)(v1 - v0 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = launch_range_gather(gd, 0, v0, v1 - v0, dpre, dstage, ctx->stream);
+    if (e == cudaSuccess && cnt > 0)
+      e = cudaMemcpyAsync(rows.data(), dstage, (size_t)cnt * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) break;
+    for (int v = v0; v < v1; ++v) {
+      const int L = live[(size_t)v];
+      const int* r = rows.data() + (pre[(size_t)v] - pre[(size_t)v0]);
+      ++gen;
+      for (int i = 0; i < L; ++i) {
+        const int u = r[i];
+        if (u < v) {
+          const int c = col[(size_t)u];
+          if (c <= L) stamp[(size_t)c] = gen;
+        }
+      }
+      int c = 0;
+      while (stamp[(size_t)c] == gen) ++c;
+      col[(size_t)v] = c;
+    }
+    v0 = v1;
+  }
+  dfree(ctx, &dpre);
+  dfree(ctx, &dstage);
+  if (e != cudaSuccess) return cuda_fail(ctx, "greedy colouring", e);
+  if (n > 0) DC_CK(cudaMemcpyAsync(ctx->color, col.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
   DC_CK(launch_color_max(graph_dev(ctx), ctx->st, ctx->stream));
   DC_CK(cudaStreamSynchronize(ctx->stream));
   return DC_OK;

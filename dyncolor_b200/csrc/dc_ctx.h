@@ -50,6 +50,7 @@ struct dc_ctx {
   unsigned* bmC = nullptr;
   int* ncolor = nullptr;
   int* sat = nullptr;
+  unsigned long long* cp = nullptr;  // HB: packed (degree property, colour) per vertex
 
   // batch scratch (sized by k and pool_cap)
   long long kcap = 0;

@@ -153,6 +153,7 @@ struct RecolorParams {
   unsigned* bmC;
   int* ncolor;           // n
   int* sat;              // n
+  unsigned long long* cp;  // HB: n packed (degree property, colour) words
   unsigned char* lflag;  // k
   // Batched mode: the graph is a disjoint union of independent graphs.
   const int* gid;        // vertex -> graph (nullptr: one graph)

@@ -138,6 +138,9 @@ struct Env {
   int variant;
   int CH;
   long long my_scanned;
+  // HB: (degree property << 32) | colour word per vertex, so one 8-byte
+  // gather gives both; the next-frontier mark lives in its colour half
+  unsigned long long* cp;
   // batched mode (all nullptr for one graph)
   const int* gid;
   int* gpush;        // HI: pushes into the next frontier per graph, this iteration
@@ -255,11 +258,16 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) ok[j] = uu[j] >= 0;
-#pragma unroll
-    for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? (g.color[uu[j]] & kColorMask) : 0;
     if (mode == M_MEX_PRIOR) {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) pp[j] = ok[j] ? g.prop[uu[j]] : 0;
+      for (int j = 0; j < 4; ++j) {
+        const unsigned long long x = ok[j] ? E.cp[uu[j]] : 0ull;
+        cc[j] = (int)((unsigned)x & (unsigned)kColorMask);
+        pp[j] = (int)(x >> 32);
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) cc[j] = ok[j] ? (g.color[uu[j]] & kColorMask) : 0;
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -337,11 +345,16 @@ __device__ void reduce_batchA(Env& E, Shared& sh, const QueueBufs& qb, long long
       pj[r] = __shfl_sync(0xffffffffu, pv, jj[r]);
       uu[r] = s < T ? g.adj[oj + (s - ej)] : -1;
     }
-#pragma unroll
-    for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? (g.color[uu[r]] & kColorMask) : 0;
     if (mode == M_MEX_PRIOR) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) pp[r] = uu[r] >= 0 ? g.prop[uu[r]] : 0;
+      for (int r = 0; r < 4; ++r) {
+        const unsigned long long x = uu[r] >= 0 ? E.cp[uu[r]] : 0ull;
+        cc[r] = (int)((unsigned)x & (unsigned)kColorMask);
+        pp[r] = (int)(x >> 32);
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) cc[r] = uu[r] >= 0 ? (g.color[uu[r]] & kColorMask) : 0;
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
@@ -415,6 +428,12 @@ __device__ __forceinline__ void flush(Env& E, PushBuf& pb, const QueueBufs& nq, 
   pb.cnt = rest;
 }
 
+// The word that holds u's next-frontier mark: its colour word (HI) or the
+// colour half of its packed word (HB).
+__device__ __forceinline__ unsigned* mark_word(const Env& E, int u) {
+  return E.cp ? reinterpret_cast<unsigned*>(E.cp + u) : reinterpret_cast<unsigned*>(E.g.color + u);
+}
+
 // Claims u for the next frontier: sets the mark bit of its colour word
 // unless the preloaded word already has it (the atomic decides races), and
 // appends the vertices this warp marked first to the warp buffer.  All
@@ -423,7 +442,7 @@ __device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, 
                                       bool want, unsigned word) {
   bool got = false;
   if (want && !(word & kMarkBit))
-    got = !(atomicOr(reinterpret_cast<unsigned*>(E.g.color + u), kMarkBit) & kMarkBit);
+    got = !(atomicOr(mark_word(E, u), kMarkBit) & kMarkBit);
   const unsigned bal = __ballot_sync(0xffffffffu, got);
   if (!bal) return;
   if (got) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = u;
@@ -461,16 +480,21 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
       const int sidx = r0 + 128 + j * 32 + lane_id();
       nx[j] = sidx < s_hi ? __ldg(g.adj + o + sidx) : -1;
     }
-    // one gather gives u's colour and its next-frontier mark
+    // one gather gives u's colour and its next-frontier mark (HB: and its
+    // degree property)
+    if (E.cp) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      ww[j] = uu[j] >= 0 ? (unsigned)g.color[uu[j]] : kMarkBit;
-      cc[j] = (int)(ww[j] & (unsigned)kColorMask);
-    }
-    if (E.variant != DC_HI) {
+      for (int j = 0; j < 4; ++j) {
+        const unsigned long long x = uu[j] >= 0 ? E.cp[uu[j]] : (unsigned long long)kMarkBit;
+        ww[j] = (unsigned)x;
+        pp[j] = (int)(x >> 32);
+      }
+    } else {
 #pragma unroll
-      for (int j = 0; j < 4; ++j) pp[j] = uu[j] >= 0 ? g.prop[uu[j]] : 0;
+      for (int j = 0; j < 4; ++j) ww[j] = uu[j] >= 0 ? (unsigned)g.color[uu[j]] : kMarkBit;
     }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) cc[j] = (int)(ww[j] & (unsigned)kColorMask);
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       mu[j] = false;
@@ -484,7 +508,7 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
     for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
   }
   const bool mv = __any_sync(0xffffffffu, markv);
-  claim(E, pb, nq, nc, v, mv && lane_id() == 0, mv ? (unsigned)ld_cg(g.color + v) : kMarkBit);
+  claim(E, pb, nq, nc, v, mv && lane_id() == 0, mv ? ld_cg(mark_word(E, v)) : kMarkBit);
 }
 
 __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long long cA, long long b,
@@ -516,15 +540,19 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
       const int ej = __shfl_sync(0xffffffffu, excl, j);
       uu[r] = s < T ? g.adj[oj + (s - ej)] : -1;
     }
+    if (E.cp) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-      ww[r] = uu[r] >= 0 ? (unsigned)g.color[uu[r]] : kMarkBit;
-      cc[r] = (int)(ww[r] & (unsigned)kColorMask);
-    }
-    if (E.variant != DC_HI) {
+      for (int r = 0; r < 4; ++r) {
+        const unsigned long long x = uu[r] >= 0 ? E.cp[uu[r]] : (unsigned long long)kMarkBit;
+        ww[r] = (unsigned)x;
+        pp[r] = (int)(x >> 32);
+      }
+    } else {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) pp[r] = uu[r] >= 0 ? g.prop[uu[r]] : 0;
+      for (int r = 0; r < 4; ++r) ww[r] = uu[r] >= 0 ? (unsigned)g.color[uu[r]] : kMarkBit;
     }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) cc[r] = (int)(ww[r] & (unsigned)kColorMask);
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       bool mu = false, mv = false;
@@ -533,7 +561,7 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
         eligible(E, R[r], uu[r], cc[r], pp[r], &mu, &mv);
       }
       claim(E, pb, nq, nc, uu[r], mu, ww[r]);
-      claim(E, pb, nq, nc, R[r].v, mv, mv ? (unsigned)ld_cg(g.color + R[r].v) : kMarkBit);
+      claim(E, pb, nq, nc, R[r].v, mv, mv ? ld_cg(mark_word(E, R[r].v)) : kMarkBit);
     }
   }
 }
@@ -605,6 +633,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
             if (E.gchg) atomicAdd(&E.gchg[E.gid[v]], 1);
           }
           g.color[v] = nc;  // also clears the frontier mark
+          if (E.cp) reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)nc;
           cmax_local = max(cmax_local, nc);
           break;
         }
@@ -615,6 +644,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           if (nc != oc) {
             if (kind == C_SEED_DEL) g.prev[v] = oc;
             g.color[v] = nc;
+            if (E.cp) reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)nc;
             cmax_local = max(cmax_local, nc);
             push = v;
           }
@@ -653,6 +683,9 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
 
 }  // namespace
 
+// One instantiation per variant, so each gets its own register allocation
+// and no per-entry variant branches.
+template <int V>
 __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   __shared__ Shared sh;
   Env E;
@@ -662,7 +695,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.p.ncolor = p.ncolor;
   E.g = p.g;
   E.st = p.st;
-  E.variant = p.variant;
+  E.variant = V;
   E.CH = p.unit_slots;
   E.my_scanned = 0;
   E.gid = p.gid;
@@ -670,6 +703,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.gchg = nullptr;
   E.gskip = nullptr;
   E.gf0 = p.gid ? p.gf0 : nullptr;
+  E.cp = V == DC_HB ? p.cp : nullptr;
   DevState* st = p.st;
   const GraphDev& g = E.g;
   unsigned bar = 0;
@@ -704,7 +738,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   if (ld_cg(&st->pre_status) != 0u) return;
 
   // ======================= seeding =======================
-  if (p.variant == DC_HI) {
+  if (V == DC_HI) {
     // D1: deletion targets (and remember which insertions had equal colours)
     for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
@@ -773,6 +807,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
                  &st->seed_targets, nullptr);
     if (!grid_sync(st, bar)) return;
   } else {
+    // packed (degree property, colour) words for this launch's gathers;
+    // the barrier after H1 publishes them before H2 reads any
+    for (long long v = gtid; v < g.n; v += gthreads)
+      E.cp[v] = ((unsigned long long)(unsigned)g.prop[v] << 32) | (unsigned)(g.color[v] & kColorMask);
     // H1: endpoints of equal-colour insertions and of all deletions
     for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
@@ -815,7 +853,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     int fb = 0;        // buffer of the frontier
     const QCount* f0c = &st->q[Q_LOOP0];
     long long it = 0;
-    const int rmode = p.variant == DC_HI ? M_MEX_ALL : M_MEX_PRIOR;
+    const int rmode = V == DC_HI ? M_MEX_ALL : M_MEX_PRIOR;
     bool go = (ld_cg(&f0c->countA) + ld_cg(&f0c->countU)) > 0;
     while (go) {
       if (it >= p.iter_cap) {
@@ -836,7 +874,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       if (p.gid) {
         int* cur = p.gcnt + (long long)ring * p.ngraphs;
         int* prv = p.gcnt + (long long)(ring ^ 1) * p.ngraphs;
-        if (p.variant == DC_HB) {
+        if (V == DC_HB) {
           // graphs with no colour change in the previous iteration are done
           // (the reference's loop would have ended for them)
           if (it > 1) {
@@ -859,7 +897,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       lap(1);
       const QCount* nc = &st->q[ns];
       const long long nq = (long long)(ld_cg(&nc->countA) + ld_cg(&nc->countU));
-      if (p.variant == DC_HI && nq == 0) break;
+      if (V == DC_HI && nq == 0) break;
       // R
       if (leader) st->chg[(it + 1) & 1] = 0;
       if (p.gid) {
@@ -867,13 +905,13 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         int* nxt = p.gcnt + (long long)(ring ^ 1) * p.ngraphs;
         for (long long gg = gtid; gg < p.ngraphs; gg += gthreads) {
           // HI: a running graph whose next frontier is empty is done
-          if (p.variant == DC_HI && p.gstate[gg] == 1 && ld_cg(&cur[gg]) == 0) {
+          if (V == DC_HI && p.gstate[gg] == 1 && ld_cg(&cur[gg]) == 0) {
             p.gstate[gg] = 2;
             p.giters[gg] = (int)it;
           }
           nxt[gg] = 0;  // next iteration's counters (last read before this phase)
         }
-        E.gchg = p.variant == DC_HB ? cur : nullptr;
+        E.gchg = V == DC_HB ? cur : nullptr;
       }
       phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
       ++ps;
@@ -884,7 +922,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
                    &st->chg[it & 1]);
       if (!grid_sync(st, bar)) return;
       lap(3);
-      if (p.variant == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;
+      if (V == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;
       fs = ns;
       fb = nb;
     }
@@ -909,15 +947,16 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
 cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s) {
   RecolorParams q = p;
   void* args[] = {&q};
-  return cudaLaunchCooperativeKernel((const void*)recolor_kernel, dim3(grid), dim3(kThreads), args,
-                                     0, s);
+  const void* fn = p.variant == DC_HB ? (const void*)recolor_kernel<DC_HB> : (const void*)recolor_kernel<DC_HI>;
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, 0, s);
 }
 
 int recolor_kernel_occupancy() {
-  int b = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recolor_kernel, kThreads, 0) != cudaSuccess)
+  int a = 0, b = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, recolor_kernel<DC_HI>, kThreads, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recolor_kernel<DC_HB>, kThreads, 0) != cudaSuccess)
     return 0;
-  return b;
+  return a < b ? a : b;
 }
 
 }  // namespace dc

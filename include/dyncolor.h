@@ -128,6 +128,13 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
 /* initial-color (read_Input_Color): colours must lie in [0, 2^30). */
 dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n);
 
+/* Initial colouring of the resident graph, not in the reference (whose
+ * initial colours come from an external tool, MG/README.txt:19-22): greedy
+ * lowest free colour in vertex-id order over the current edge set.  The
+ * rows are read back to the host and coloured there, since the greedy order
+ * is serial; the result equals dcg_greedy_color on the same edges. */
+dc_status dc_colors_init_greedy(dc_ctx* ctx);
+
 /* apply-update-batch from host memory (any host pointer; pinned is fastest).
  * Validates every line first (DC_E_INVAL leaves the state untouched).  Runs
  * the structural update and the recolouring on the context's stream and

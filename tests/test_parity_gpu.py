@@ -286,3 +286,25 @@ def test_cuda_graph_replay_matches_oracle(variant, ov):
         sg = ctx.apply_batch(to_dc_changes(ch))
         check_same(ctx, g, sg, so)
     ctx.close()
+
+
+def test_greedy_initial_colouring_of_the_resident_graph():
+    n, a, b = rmat_graph(12, seed=4)
+    ctx = dc.Context(variant=dc.HI, unit_slots=256)
+    ctx.load_edges(n, a, b)
+    ctx.init_greedy_colors()
+    want = dc.greedy_color(n, a, b)
+    assert np.array_equal(ctx.colors(), want)
+    assert ctx.validate() == 0
+    # after a batch the colouring follows the current edge set
+    es = dc.EdgeSet(n, a, b)
+    ch = es.sample_batch(3000, 3000, seed=5)
+    ctx.apply_batch(ch)
+    rows = [ctx.neighbors(v) for v in range(n)]
+    x = np.concatenate([np.full(len(r), v, np.int32) for v, r in enumerate(rows)])
+    y = np.concatenate(rows).astype(np.int32)
+    keep = x < y
+    ctx.init_greedy_colors()
+    assert np.array_equal(ctx.colors(), dc.greedy_color(n, x[keep], y[keep]))
+    assert ctx.validate() == 0
+    ctx.close()
