@@ -56,6 +56,8 @@ def parse_args():
                     help="change lines of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-iter-cap", type=int, default=400)
+    ap.add_argument("--unit-slots", type=int, default=0, help="adjacency slots per warp work unit (0: library default)")
+    ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent CTAs per SM (0: from occupancy)")
     ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
                     help="plain: one large graph (headline); batched: many graphs in one launch; "
                          "served: request stream over resident graphs")
@@ -348,7 +350,8 @@ def run_ours(args, dist: Dist):
     w = get_workload(args, dist, W + 2 * K)
     variant = dc.HI if args.variant == "hi" else dc.HB
     stream = torch.cuda.Stream(device=dev)
-    ctx = dc.Context(variant=variant, device=dev, stream=stream.cuda_stream)
+    ctx = dc.Context(variant=variant, device=dev, stream=stream.cuda_stream, unit_slots=args.unit_slots,
+                     blocks_per_sm=args.blocks_per_sm)
     t0 = time.time()
     ctx.load_edges(w["n"], w["a"], w["b"])
     ctx.set_colors(w["colors"])
