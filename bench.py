@@ -78,20 +78,30 @@ def parse_args():
 # ---------------------------------------------------------------------------
 
 class Dist:
-    def __init__(self, want_gpus: int):
+    """One process per GPU (torchrun env).  NCCL on GPUs; gloo with CPU
+    tensors where no GPU is visible (the multi-process host logic)."""
+
+    def __init__(self, want_gpus: int, backend: str | None = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = False
+        self.dev = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as tdist
 
-            torch.cuda.set_device(self.local)
-            tdist.init_process_group("nccl", timeout=datetime.timedelta(minutes=10),
-                                     device_id=torch.device("cuda", self.local))
+            backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+            timeout = datetime.timedelta(minutes=10)
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.dev = torch.device("cuda", self.local)
+                tdist.init_process_group("nccl", timeout=timeout, device_id=self.dev)
+            else:
+                self.dev = torch.device("cpu")
+                tdist.init_process_group("gloo", timeout=timeout)
             self.pg = True
 
     def barrier(self):
@@ -100,25 +110,27 @@ class Dist:
 
             tdist.barrier()
 
-    def max(self, x: float) -> float:
-        if not self.pg:
-            return x
+    def _reduce(self, x: float, op) -> float:
         import torch
         import torch.distributed as tdist
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+        t = torch.tensor([x], dtype=torch.float64, device=self.dev)
+        tdist.all_reduce(t, op=op)
         return float(t.item())
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch.distributed as tdist
+
+        return self._reduce(x, tdist.ReduceOp.MAX)
 
     def sum(self, x: float) -> float:
         if not self.pg:
             return x
-        import torch
         import torch.distributed as tdist
 
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        tdist.all_reduce(t, op=tdist.ReduceOp.SUM)
-        return float(t.item())
+        return self._reduce(x, tdist.ReduceOp.SUM)
 
     def close(self):
         if self.pg:
