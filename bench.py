@@ -692,6 +692,7 @@ def run_served(args):
                 "restores": info1["restores"] - info0["restores"], "spills": info1["spills"] - info0["spills"],
                 "restore_ms": round(info1["restore_ms"] - info0["restore_ms"], 1),
                 "spill_ms": round(info1["spill_ms"] - info0["spill_ms"], 1),
+                "compact_ms": round(info1["compact_ms"] - info0["compact_ms"], 1),
                 "compactions": info1["compactions"] - info0["compactions"],
                 "device_gb": round(info1["device_bytes"] / 1e9, 2),
                 "pinned_host_gb": round(info1["host_bytes"] / 1e9, 2),

@@ -289,9 +289,18 @@ dc_status repack(dc_ctx* ctx, long long new_cap) {
     dfree(ctx, &len2);
     dfree(ctx, &adj2);
   };
-  if ((s = dalloc(ctx, &off2, n, "repack offsets")) != DC_OK || (s = dalloc(ctx, &cap2, n, "repack caps")) != DC_OK ||
-      (s = dalloc(ctx, &len2, n, "repack lengths")) != DC_OK ||
-      (s = dalloc(ctx, &adj2, new_cap, "repack pool")) != DC_OK) {
+  // a context that compacts often keeps the previous arrays as the next
+  // compaction's target instead of freeing and reallocating gigabytes
+  if (ctx->keep_spare && ctx->spare.adj && ctx->spare.adj_cap >= new_cap) {
+    off2 = ctx->spare.off;
+    cap2 = ctx->spare.cap;
+    len2 = ctx->spare.len;
+    adj2 = ctx->spare.adj;
+    ctx->spare = dc_ctx::Spare{};
+  } else if ((s = dalloc(ctx, &off2, n, "repack offsets")) != DC_OK ||
+             (s = dalloc(ctx, &cap2, n, "repack caps")) != DC_OK ||
+             (s = dalloc(ctx, &len2, n, "repack lengths")) != DC_OK ||
+             (s = dalloc(ctx, &adj2, new_cap, "repack pool")) != DC_OK) {
     drop();
     return s;
   }
@@ -307,10 +316,22 @@ dc_status repack(dc_ctx* ctx, long long new_cap) {
   DC_CK(cudaMemcpyAsync(&ctx->st->pool_used, ctx->h_scalar + 1, 8, cudaMemcpyHostToDevice, ctx->stream));
   DC_CK(cudaStreamSynchronize(ctx->stream));
   dfree(ctx, &scratch);
-  dfree(ctx, &ctx->off);
-  dfree(ctx, &ctx->cap);
-  dfree(ctx, &ctx->len);
-  dfree(ctx, &ctx->adj);
+  if (ctx->keep_spare) {
+    dfree(ctx, &ctx->spare.off);  // a spare too small for this compaction
+    dfree(ctx, &ctx->spare.cap);
+    dfree(ctx, &ctx->spare.len);
+    dfree(ctx, &ctx->spare.adj);
+    ctx->spare.off = ctx->off;
+    ctx->spare.cap = ctx->cap;
+    ctx->spare.len = ctx->len;
+    ctx->spare.adj = ctx->adj;
+    ctx->spare.adj_cap = ctx->pool_cap;
+  } else {
+    dfree(ctx, &ctx->off);
+    dfree(ctx, &ctx->cap);
+    dfree(ctx, &ctx->len);
+    dfree(ctx, &ctx->adj);
+  }
   ctx->off = off2;
   ctx->cap = cap2;
   ctx->len = len2;
@@ -598,6 +619,10 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->cap);
   dfree(ctx, &ctx->live);
   dfree(ctx, &ctx->adj);
+  dfree(ctx, &ctx->spare.off);
+  dfree(ctx, &ctx->spare.cap);
+  dfree(ctx, &ctx->spare.len);
+  dfree(ctx, &ctx->spare.adj);
   dfree(ctx, &ctx->color);
   dfree(ctx, &ctx->prev);
   dfree(ctx, &ctx->prop);

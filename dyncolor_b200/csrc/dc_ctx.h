@@ -29,6 +29,14 @@ struct dc_ctx {
   int key_bits = 1;
   long long pool_cap = 0;
   long long max_pool_cap = 0;  // > 0: pool growth stops here (a resident pool's budget)
+  bool keep_spare = false;      // compactions reuse the previous arrays (resident pools)
+  struct Spare {
+    long long* off = nullptr;
+    int* cap = nullptr;
+    int* len = nullptr;
+    int* adj = nullptr;
+    long long adj_cap = 0;
+  } spare;
   long long* off = nullptr;
   int* len = nullptr;
   int* cap = nullptr;

@@ -197,6 +197,7 @@ dc_status read_used(dc_pool* P, long long* used) {
 // when the graphs that must stay resident need more.
 dc_status compact(dc_pool* P, long long extra) {
   dc_ctx* ctx = P->u;
+  const double t0 = now_ms();
   long long T = 0;
   dc_status s = packed_total(ctx, &T, nullptr);
   if (s != DC_OK) return s;
@@ -209,6 +210,7 @@ dc_status compact(dc_pool* P, long long extra) {
   if (target > P->budget) ++P->info.overbudget;
   ++P->info.compactions;
   DC_CK(cudaStreamSynchronize(ctx->stream));
+  P->info.compact_ms += now_ms() - t0;
   return DC_OK;
 }
 
@@ -238,6 +240,28 @@ dc_status upload_prerel(dc_pool* P, const long long* pre, int v0, int v1) {
   return DC_OK;
 }
 
+// The graph's pinned host slot: per-vertex arrays, and rows for at least
+// `rows` ids.  Rows grow by half again when they outgrow the slot, so a
+// graph that keeps growing is not re-pinned at every spill (pinning costs
+// far more per byte than copying).
+dc_status host_slot(dc_pool* P, PGraph& g, long long rows) {
+  dc_status s;
+  const int n = g.n;
+  if (!g.h_color) {
+    if ((s = halloc(P, &g.h_color, n)) != DC_OK) return s;
+    if ((s = halloc(P, &g.h_prev, n)) != DC_OK) return s;
+    if ((s = halloc(P, &g.h_prop, n)) != DC_OK) return s;
+    if ((s = halloc(P, &g.h_live, n)) != DC_OK) return s;
+    if ((s = halloc(P, &g.h_pre, (long long)n + 1)) != DC_OK) return s;
+  }
+  if (rows > g.rows_cap) {
+    const long long cap = std::max(rows, g.rows_cap + g.rows_cap / 2);
+    if ((s = halloc(P, &g.h_rows, cap)) != DC_OK) return s;
+    g.rows_cap = cap;
+  }
+  return DC_OK;
+}
+
 // Moves a resident graph to pinned host memory and frees its vertex ids.
 dc_status spill(dc_pool* P, int gi) {
   dc_ctx* ctx = P->u;
@@ -246,13 +270,7 @@ dc_status spill(dc_pool* P, int gi) {
   const double t0 = now_ms();
   const int f = g.first, n = g.n;
   dc_status s;
-  if (!g.h_color) {
-    if ((s = halloc(P, &g.h_color, n)) != DC_OK) return s;
-    if ((s = halloc(P, &g.h_prev, n)) != DC_OK) return s;
-    if ((s = halloc(P, &g.h_prop, n)) != DC_OK) return s;
-    if ((s = halloc(P, &g.h_live, n)) != DC_OK) return s;
-    if ((s = halloc(P, &g.h_pre, (long long)n + 1)) != DC_OK) return s;
-  }
+  if ((s = host_slot(P, g, 0)) != DC_OK) return s;
   const size_t nb = (size_t)n * 4;
   if (n > 0) {
     DC_CK(cudaMemcpyAsync(g.h_live, ctx->live + f, nb, cudaMemcpyDeviceToHost, ctx->stream));
@@ -270,10 +288,7 @@ dc_status spill(dc_pool* P, int gi) {
     maxc = std::max(maxc, g.h_color[v]);
   }
   const long long S = g.h_pre[n];
-  if (S > g.rows_cap) {
-    if ((s = halloc(P, &g.h_rows, S)) != DC_OK) return s;
-    g.rows_cap = S;
-  }
+  if ((s = host_slot(P, g, S)) != DC_OK) return s;
   const GraphDev gd = graph_dev(ctx);
   for (int v0 = 0; v0 < n;) {
     int v1 = v0;
@@ -492,6 +507,7 @@ dc_status dc_pool_create(dc_pool** out, const dc_pool_options* opt) {
   P->budget = (o.pool_slots + 3) & ~3ll;
   P->hard = std::max(P->budget, (o.pool_slots_max > 0 ? o.pool_slots_max : 2 * o.pool_slots) & ~3ll);
   ctx->max_pool_cap = P->budget;
+  ctx->keep_spare = true;  // a pool compacts often
   if ((s = dc_graph_load_edges(ctx, o.vertex_capacity, nullptr, nullptr, 0)) != DC_OK) return bail(s);
   P->G = o.max_graphs;
   const long long G1 = (long long)P->G + 1;
@@ -622,6 +638,11 @@ dc_status dc_pool_add_graph(dc_pool* P, int32_t n, const int32_t* a, const int32
   long long packed = 0;
   for (int v = 0; v < n; ++v) packed += packed_cap_host(live[(size_t)v], ctx->opt.slack);
   g.packed = packed;
+  // the host slot is pinned now, while the graph is registered, not at its
+  // first spill in the middle of serving
+  long long live_total = 0;
+  for (int v = 0; v < n; ++v) live_total += live[(size_t)v];
+  if ((s = host_slot(P, g, live_total + live_total / 4)) != DC_OK) return s;
   int cmax = 0;
   std::memcpy(&cmax, ctx->h_scalar, 4);
   if (maxc > cmax) {

@@ -64,6 +64,7 @@ class PoolInfo(C.Structure):
         ("compactions", C.c_int64),
         ("device_bytes", C.c_int64),
         ("host_bytes", C.c_int64),
+        ("compact_ms", C.c_double),
     ]
 
     def as_dict(self):

@@ -87,6 +87,7 @@ typedef struct {
   int64_t compactions;
   int64_t device_bytes;    /* device memory held by the pool */
   int64_t host_bytes;      /* pinned host memory held by the pool */
+  double compact_ms;       /* host wall time inside compactions */
 } dc_pool_info;
 
 dc_status dc_pool_options_default(dc_pool_options* opt);
