@@ -56,6 +56,10 @@ def parse_args():
                     help="change lines of the bounded CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-iter-cap", type=int, default=400)
+    ap.add_argument("--ref-sample", type=int, default=5_000,
+                    help="reference arm: change lines of each step's bounded sample")
+    ap.add_argument("--ref-step-budget-ms", type=float, default=5_000.0,
+                    help="reference arm: a step's loop stops once its timed work passes this budget")
     ap.add_argument("--unit-slots", type=int, default=0, help="adjacency slots per warp work unit (0: library default)")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent CTAs per SM (0: from occupancy)")
     ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
@@ -319,11 +323,12 @@ def run_reference(args, dist: Dist) -> dict:
         files = []
         for i in range(nb):
             f = os.path.join(d, f"x{i}.txt")
-            po.write_change_file(f, w["batches"][i][: args.cpu_sample])
+            po.write_change_file(f, w["batches"][i][: args.ref_sample])
             files.append(f)
         out = os.path.join(d, "o.txt")
         subprocess.run([exe, "bench", os.path.join(d, "g.bin"), str(w["n"]), str(len(w["a"])),
-                        os.path.join(d, "c.bin"), ",".join(files), out, str(args.ref_iter_cap)],
+                        os.path.join(d, "c.bin"), ",".join(files), out, str(args.ref_iter_cap),
+                        str(args.ref_step_budget_ms)],
                        check=True, stdout=subprocess.DEVNULL)
         rows = [line.split() for line in open(out)]
     finally:
@@ -332,11 +337,13 @@ def run_reference(args, dist: Dist) -> dict:
     ms = sum(float(r[5]) for r in timed)
     its = [int(r[1]) for r in timed]
     capped = sum(1 for r in timed if r[3] != "0")
-    lines = args.cpu_sample * len(timed)
+    lines = args.ref_sample * len(timed)
     value = lines / (ms / 1e3)
-    sample = (f"first {args.cpu_sample} lines of each of {len(timed)} batches, each applied to the "
+    sample = (f"first {args.ref_sample} lines of each of {len(timed)} batches, each applied to the "
               f"initial graph by the reference's own kernel bodies run serially on 1 host core "
-              f"(iterations {its}, {capped} stopped at the {args.ref_iter_cap}-iteration cap; the "
+              f"(loop iterations {its}; {capped} of {len(timed)} steps stopped at the "
+              f"{args.ref_iter_cap}-iteration cap or the {args.ref_step_budget_ms / 1e3:.0f} s step budget "
+              f"before the recolouring converged, so the value overstates the reference; the "
               f"reference's 32-bit masks are exact only for colours <= 30)")
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": dist.world,
@@ -475,11 +482,12 @@ def run_ours(args, dist: Dist):
 # batched mode: thousands of independent graphs, one launch per update round
 # ---------------------------------------------------------------------------
 
-def build_batched_workload(count, seed, nmin=1_000, nmax=200_000, kmin=100, kmax=50_000):
+def build_batched_workload(count, seed, nmin=1_000, nmax=200_000, kmin=100, kmax=50_000, rank=0, world=1):
     """Graphs with vertex counts log-uniform in [nmin, nmax], average degree
     uniform in [8, 32], R-MAT or Erdos-Renyi (alternating), greedy colouring;
     one batch per graph of log-uniform size in [kmin, kmax], half deletions of
-    existing edges, half insertions of absent pairs."""
+    existing edges, half insertions of absent pairs.  With world > 1 only the
+    graphs i with i % world == rank are built (whole graphs per GPU)."""
     import dyncolor_b200 as dc
 
     from concurrent.futures import ThreadPoolExecutor
@@ -504,18 +512,23 @@ def build_batched_workload(count, seed, nmin=1_000, nmax=200_000, kmin=100, kmax
 
     # the generators release the GIL (ctypes), so host threads overlap them
     with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
-        out = list(ex.map(one, range(count)))
+        out = list(ex.map(one, range(rank, count, world)))
     return [o[0] for o in out], [o[1] for o in out], [o[2] for o in out]
 
 
-def run_batched(args):
+def run_batched(args, dist):
     import dyncolor_b200 as dc
     from dyncolor_b200.batched import BatchedContext
     from dyncolor_b200.tune import autotune
 
     variant = dc.HI if args.variant == "hi" else dc.HB
     t0 = time.time()
-    graphs, colors, batches = build_batched_workload(args.graphs, args.seed)
+    import torch
+
+    torch.cuda.set_device(dist.local)
+    dev = dist.local
+    # whole graphs per GPU: rank r takes graphs r, r + N, ...
+    graphs, colors, batches = build_batched_workload(args.graphs, args.seed, rank=dist.rank, world=dist.world)
     gen_s = time.time() - t0
     lines = int(sum(len(x) for x in batches))
     # autotune the tile parameters on a sample of the graphs
@@ -524,21 +537,23 @@ def run_batched(args):
     sg, sc, sb = [graphs[i] for i in idx], [colors[i] for i in idx], [batches[i] for i in idx]
 
     def make(opts):
-        bc = BatchedContext(variant=variant, **opts)
+        bc = BatchedContext(variant=variant, device=dev, **opts)
         bc.load(sg)
         bc.set_colors(sc)
         return bc
 
     best, table = autotune(make, lambda bc: bc.apply(sb).device_ms)
     # all graphs, one launch (replayed from a captured CUDA graph)
-    bc = BatchedContext(variant=variant, cuda_graph=True, **best)
+    bc = BatchedContext(variant=variant, device=dev, cuda_graph=True, **best)
     bc.load(graphs)
     bc.set_colors(colors)
     ub = bc.union_batch(batches)
+    dist.barrier()
     t0 = time.perf_counter()
     st = bc.ctx.apply_batch(ub)
     got = bc.ctx.colors()
-    e2e_b = time.perf_counter() - t0
+    e2e_b = dist.max(time.perf_counter() - t0)
+    dev_b = dist.max(st.device_ms)
     its_b = bc.iterations()
     first = bc.first.copy()
     bc.close()
@@ -546,7 +561,7 @@ def run_batched(args):
     dev_plain, e2e_p, its_p = 0.0, 0.0, []
     mismatched = 0
     for g, ((n, a, b), c0, x) in enumerate(zip(graphs, colors, batches)):
-        pc = dc.Context(variant=variant, **best)
+        pc = dc.Context(variant=variant, device=dev, **best)
         pc.load_edges(n, a, b)
         pc.set_colors(c0)
         t0 = time.perf_counter()
@@ -558,22 +573,31 @@ def run_batched(args):
         its_p.append(s1.iterations)
         if not np.array_equal(alone, got[first[g]:first[g + 1]]):
             mismatched += 1
-    same = mismatched == 0 and bool(np.array_equal(its_b, np.array(its_p)))
-    value = lines / (st.device_ms / 1e3)
-    plain = lines / (dev_plain / 1e3)
+    same_local = mismatched == 0 and bool(np.array_equal(its_b, np.array(its_p)))
+    # every rank ran its own graphs at the same time: max of the times, sum of the work
+    lines_all = int(dist.sum(float(lines)))
+    mismatched = int(dist.sum(float(mismatched)))
+    same = dist.sum(0.0 if same_local else 1.0) == 0.0
+    dev_plain = dist.max(dev_plain)
+    e2e_p = dist.max(e2e_p)
+    nverts = int(dist.sum(float(first[-1])))
+    nedges = int(dist.sum(float(sum(len(x) for _, x, _ in graphs))))
+    value = lines_all / (dev_b / 1e3)
+    plain = lines_all / (dev_plain / 1e3)
+    lines = lines_all
     return {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
-        "ms_per_step": st.device_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": 1, "warmup": 0,
+        "ms_per_step": dev_b, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic", "mode": "batched",
-        "config": {"workload": (f"{len(graphs)} independent graphs (vertices log-uniform in [1k, 200k], "
+        "config": {"workload": (f"{args.graphs} independent graphs (vertices log-uniform in [1k, 200k], "
                                 f"average degree uniform in [8, 32], R-MAT / Erdos-Renyi alternating), one "
                                 f"batch per graph (log-uniform in [100, 50k] lines, 50/50), variant "
                                 f"{args.variant.upper()}"),
-                   "vertices": int(first[-1]), "edges": int(sum(len(x) for _, x, _ in graphs)),
-                   "lines": lines, "tuned": best, "cuda_graph": True},
+                   "vertices": nverts, "edges": nedges, "lines": lines, "tuned": best, "cuda_graph": True,
+                   "parallelism": f"whole graphs per GPU over {dist.world} GPU(s)"},
         "e2e": {"value": lines / e2e_b, "unit": UNIT, "h2d_bytes_per_step": 12 * lines,
-                "d2h_bytes_per_step": 4 * int(first[-1])},
-        "plain_each_graph_alone": {"value": plain, "e2e": lines / e2e_p, "launches": 2 * len(graphs),
+                "d2h_bytes_per_step": 4 * nverts},
+        "plain_each_graph_alone": {"value": plain, "e2e": lines / e2e_p, "launches": 2 * args.graphs,
                                    "device_ms": dev_plain},
         "speedup_vs_plain": value / plain,
         "bit_exact_vs_alone": same, "graphs_differing": mismatched,
@@ -727,7 +751,13 @@ def run_served(args):
 def main():
     args = parse_args()
     if args.mode == "batched":
-        print(json.dumps(run_batched(args)), flush=True)
+        dist = Dist(args.gpus)
+        try:
+            out = run_batched(args, dist)
+            if dist.rank == 0:
+                print(json.dumps(out), flush=True)
+        finally:
+            dist.close()
         return
     if args.mode == "served":
         print(json.dumps(run_served(args)), flush=True)

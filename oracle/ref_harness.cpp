@@ -28,7 +28,9 @@
  * out: "iterations <n> status <0|4>\n" then one colour per line.
  *
  * Timing mode (serial schedule, for the CPU baseline of the benchmark):
- *   ref_{hi,hb} bench graph.bin nodes edges colors.bin ch1[,ch2,...] out [iter_cap]
+ *   ref_{hi,hb} bench graph.bin nodes edges colors.bin ch1[,ch2,...] out [iter_cap [budget_ms]]
+ *   (a step stops at iter_cap loop iterations or once its timed work passes
+ *   budget_ms, with status 4, so a timing run ends in bounded time)
  * graph.bin holds int32 pairs (a0 b0 a1 b1 ...) turned into the adjacency the
  * way read_graphEdges does; colors.bin holds one int32 per vertex.  Every
  * change file is one step applied to the initial graph and colouring (the
@@ -125,7 +127,8 @@ struct StepResult {
 
 // One update batch as the reference driver applies it
 // (HI/Color_main.cu:62-202, HB/Color_main.cu:71-224).
-StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long iter_cap) {
+StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long iter_cap,
+                    double budget_ms = 0.0) {
   using clk = std::chrono::steady_clock;
   StepResult R;
   const int nodes = G.nodes;
@@ -216,7 +219,9 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
   long it = 0;
   counter = compact(S, list);
   while (ok && S.change > 0) {
-    if (it >= iter_cap) {
+    // the iteration cap, or (timing mode) the time budget of the step
+    if (it >= iter_cap ||
+        (budget_ms > 0 && std::chrono::duration<double, std::milli>(clk::now() - t0).count() + R.ms > budget_ms)) {
       R.status = 4;
       break;
     }
@@ -271,6 +276,7 @@ int main(int argc, char* argv[]) {
   const bool snapshot = std::strcmp(argv[1], "snapshot") == 0;
   const int nodes = std::atoi(argv[3]);
   const long iter_cap = argc > 8 ? std::atol(argv[8]) : 100000;
+  const double budget_ms = argc > 9 ? std::atof(argv[9]) : 0.0;  // bench mode: per-step time budget
   Graph G;
   G.nodes = nodes;
   G.adj.resize(nodes);
@@ -350,7 +356,7 @@ int main(int argc, char* argv[]) {
       }
       std::fclose(cf);
     }
-    const StepResult R = run_step(G, S, file.c_str(), false, iter_cap);
+    const StepResult R = run_step(G, S, file.c_str(), false, iter_cap, budget_ms);
     std::fprintf(f, "iterations %ld status %d time_ms %.3f\n", R.iterations, R.status, R.ms);
     std::fflush(f);
     for (auto it = sizes.rbegin(); it != sizes.rend(); ++it) G.adj[it->first].resize(it->second);
