@@ -68,6 +68,22 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     q.capU = capU;
     q.capM = capM;
   }
+  if (ctx->opt.variant == DC_HI && ctx->opt.heavy_min_live > 0) {
+    // heavy-row index: rows that do not fit lose their index (and are scanned in full)
+    HriBufs& h = ctx->hri;
+    h.min_live = ctx->opt.heavy_min_live;
+    h.cap_rows = ctx->pool_cap / h.min_live + 1;
+    h.cap_pairs = ctx->pool_cap / 8 + 4096;
+    h.cap_exc = h.cap_pairs / 4 + 64 * h.cap_rows;
+    h.cap_a = n / 8 + ctx->pool_cap / CH + 1024;
+    if ((s = dalloc(ctx, &h.hrow, h.cap_rows, "heavy rows")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.hoff, h.cap_rows + 1, "heavy-row offsets")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.xoff, h.cap_rows + 1, "change-list offsets")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.xcnt, h.cap_rows, "change-list counts")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.pairs, h.cap_pairs, "ordered neighbours")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.xv, h.cap_exc, "change lists")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.alist, h.cap_a, "append queue")) != DC_OK) return s;
+  }
   if (!ctx->bmA) {
     if ((s = dalloc(ctx, &ctx->bmA, words, "bitmap")) != DC_OK) return s;
     if ((s = dalloc(ctx, &ctx->bmB, words, "bitmap")) != DC_OK) return s;
@@ -75,6 +91,11 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     if ((s = dalloc(ctx, &ctx->ncolor, n, "ncolor")) != DC_OK) return s;
     if ((s = dalloc(ctx, &ctx->sat, n, "sat")) != DC_OK) return s;
     if (ctx->opt.variant == DC_HB && (s = dalloc(ctx, &ctx->cp, n, "packed words")) != DC_OK) return s;
+    if (ctx->opt.variant == DC_HI && ctx->opt.heavy_min_live > 0) {
+      HriBufs& h = ctx->hri;
+      if ((s = dalloc(ctx, &h.hid, n, "heavy-row ids")) != DC_OK) return s;
+      if ((s = dalloc(ctx, &h.bmF, words, "changed-colour bitmap")) != DC_OK) return s;
+    }
     DC_CK(cudaMemsetAsync(ctx->bmA, 0, words * 4, ctx->stream));
     DC_CK(cudaMemsetAsync(ctx->bmB, 0, words * 4, ctx->stream));
     DC_CK(cudaMemsetAsync(ctx->bmC, 0, words * 4, ctx->stream));
@@ -212,6 +233,7 @@ RecolorParams recolor_params(dc_ctx* ctx, const dc_change* ch, long long k) {
   p.ncolor = ctx->ncolor;
   p.sat = ctx->sat;
   p.cp = ctx->cp;
+  p.hri = ctx->hri;
   p.lflag = ctx->lflag;
   if (ctx->ngraphs > 0) {
     p.gid = ctx->gid;
@@ -370,6 +392,7 @@ dc_status enqueue_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const
     const size_t b0 = offsetof(DevState, bar_arrived);
     const size_t b1 = offsetof(DevState, wctr) + sizeof(((DevState*)nullptr)->wctr);
     DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
+    if (ctx->hri.min_live > 0) DC_CK(launch_hri_build(graph_dev(ctx), ctx->hri, ctx->st, ctx->stream));
     RecolorParams rp = recolor_params(ctx, d_ch, k);
     rp.k_dev = k_dev;
     DC_CK(launch_recolor(rp, ctx->grid_recolor, ctx->stream));
@@ -537,6 +560,7 @@ dc_status dc_options_default(dc_options* opt) {
   opt->blocks_per_sm = 0;
   opt->reserve_slots = 0;
   opt->unit_slots = kUnitSlotsDefault;
+  opt->heavy_min_live = kHeavyMinLive;
   return DC_OK;
 }
 
@@ -553,6 +577,9 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   if (!(o.slack > 1.0f)) o.slack = 1.25f;
   if (o.unit_slots <= 0) o.unit_slots = kUnitSlotsDefault;
   if (o.unit_slots % 128 != 0 || o.unit_slots < 128) return DC_E_INVAL;
+  if (o.heavy_min_live == 0) o.heavy_min_live = kHeavyMinLive;
+  if (o.heavy_min_live < 0 || o.variant != DC_HI) o.heavy_min_live = 0;  // off
+  if (o.heavy_min_live > 0 && o.heavy_min_live < 64) o.heavy_min_live = 64;
   dc_ctx* ctx = new (std::nothrow) dc_ctx();
   if (!ctx) return DC_E_NOMEM;
   ctx->opt = o;
@@ -614,6 +641,15 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->ncolor);
   dfree(ctx, &ctx->sat);
   dfree(ctx, &ctx->cp);
+  dfree(ctx, &ctx->hri.hid);
+  dfree(ctx, &ctx->hri.bmF);
+  dfree(ctx, &ctx->hri.hrow);
+  dfree(ctx, &ctx->hri.hoff);
+  dfree(ctx, &ctx->hri.xoff);
+  dfree(ctx, &ctx->hri.xcnt);
+  dfree(ctx, &ctx->hri.pairs);
+  dfree(ctx, &ctx->hri.xv);
+  dfree(ctx, &ctx->hri.alist);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->len);
   dfree(ctx, &ctx->cap);

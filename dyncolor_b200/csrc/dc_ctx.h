@@ -11,6 +11,7 @@
 
 using dc::DevState;
 using dc::QueueBufs;
+using dc::HriBufs;
 
 struct dc_ctx {
   dc_options opt{};
@@ -59,6 +60,7 @@ struct dc_ctx {
   int* ncolor = nullptr;
   int* sat = nullptr;
   unsigned long long* cp = nullptr;  // HB: packed (degree property, colour) per vertex
+  HriBufs hri{};                     // HI: heavy-row index (min_live 0: off)
 
   // batch scratch (sized by k and pool_cap)
   long long kcap = 0;

@@ -1,0 +1,158 @@
+// dc_hri.cu -- heavy-row index of the HI recolouring loop, rebuilt before
+// every recolour launch (after the structural update of the batch).
+//
+//   classify  rows with at least min_live live slots get an index i (in
+//             arrival order; the order never affects results) and clear the
+//             changed-colour bitmap
+//   offsets   one CTA: exclusive scans of the rows' live counts (ordered
+//             copies) and of their change-list capacities; rows past the
+//             buffers' capacity lose their index and are scanned in full
+//   fill      one CTA per row: counting sort of the row's live neighbours
+//             by colour, descending (colours >= kHriBins - 1 share the first
+//             bin), written as (colour << 32) | neighbour
+#include "dc_device.cuh"
+
+namespace dc {
+
+namespace {
+
+constexpr int kHriThreads = 512;
+
+__device__ __forceinline__ int hri_bin(int c) { return c < kHriBins - 1 ? c : kHriBins - 1; }
+
+// Change-list capacity of a row with `live` slots.
+__device__ __forceinline__ long long xcap(int live) { return live / 4 + 64; }
+
+__global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
+  const long long nt = (long long)gridDim.x * blockDim.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (long long v = t; v < g.n; v += nt) {
+    int id = -1;
+    if (g.live[v] >= h.min_live) {
+      const unsigned long long i = atomicAdd(&st->hcount, 1ull);
+      if ((long long)i < h.cap_rows) {
+        id = (int)i;
+        h.hrow[i] = (int)v;
+      }
+    }
+    h.hid[v] = id;
+  }
+  const long long words = ((long long)g.n + 31) / 32 + 1;
+  for (long long w = t; w < words; w += nt) h.bmF[w] = 0u;
+}
+
+// Single CTA.  hoff / xoff get exclusive prefixes; rows whose copy or list
+// would pass the buffers lose their index.
+__global__ void hri_offsets_kernel(GraphDev g, HriBufs h, DevState* st) {
+  __shared__ long long sw[kHriThreads / 32];
+  __shared__ long long s_tot[2];
+  const long long R = min((long long)ld_cg(&st->hcount), h.cap_rows);
+  long long run_p = 0, run_x = 0;
+  for (long long c0 = 0; c0 < R; c0 += kHriThreads) {
+    const long long i = c0 + threadIdx.x;
+    const int L = i < R ? g.live[h.hrow[i]] : 0;
+    const long long xp = i < R ? xcap(L) : 0;
+    // two block scans (pairs, list capacity)
+    long long vals[2] = {(long long)L, xp};
+    long long excl[2];
+    for (int k = 0; k < 2; ++k) {
+      long long incl = vals[k];
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane_id() >= o) incl += y;
+      }
+      if (lane_id() == 31) sw[warp_id()] = incl;
+      __syncthreads();
+      long long wbase = 0, tot = 0;
+      for (int w = 0; w < kHriThreads / 32; ++w) {
+        if (w < warp_id()) wbase += sw[w];
+        tot += sw[w];
+      }
+      excl[k] = wbase + incl - vals[k];
+      if (threadIdx.x == 0) s_tot[k] = tot;
+      __syncthreads();
+    }
+    if (i < R) {
+      const long long po = run_p + excl[0], xo = run_x + excl[1];
+      h.hoff[i] = po;
+      h.xoff[i] = xo;
+      h.xcnt[i] = 0;
+      if (po + L > h.cap_pairs || xo + xp > h.cap_exc) h.hid[h.hrow[i]] = -1;  // no room: full scans
+    }
+    run_p += s_tot[0];
+    run_x += s_tot[1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    h.hoff[R] = min(run_p, h.cap_pairs);
+    h.xoff[R] = min(run_x, h.cap_exc);
+  }
+}
+
+__global__ void __launch_bounds__(kHriThreads) hri_fill_kernel(GraphDev g, HriBufs h, DevState* st) {
+  __shared__ int hist[kHriBins];
+  __shared__ int sw[kHriThreads / 32 + 1];
+  const long long R = min((long long)ld_cg(&st->hcount), h.cap_rows);
+  for (long long i = blockIdx.x; i < R; i += gridDim.x) {
+    const int v = h.hrow[i];
+    if (h.hid[v] != (int)i) continue;  // lost its index in the offsets pass (uniform per CTA)
+    const long long o = g.off[v];
+    const int L = g.len[v];
+    const long long base = h.hoff[i];
+    const long long room = h.hoff[i + 1] - base;  // == live[v]
+    for (int b = threadIdx.x; b < kHriBins; b += kHriThreads) hist[b] = 0;
+    __syncthreads();
+    for (int s = threadIdx.x; s < L; s += kHriThreads) {
+      const int u = g.adj[o + s];
+      if (u >= 0) atomicAdd(&hist[hri_bin(g.color[u] & kColorMask)], 1);
+    }
+    __syncthreads();
+    // descending bins: start of bin b = sum of the counts of bins above b.
+    // Thread t owns bins [2t, 2t + 1] counted from the top.
+    {
+      const int b0 = kHriBins - 1 - 2 * threadIdx.x, b1 = b0 - 1;
+      const int c0 = hist[b0], c1 = hist[b1];
+      int incl = c0 + c1;
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane_id() >= off) incl += y;
+      }
+      if (lane_id() == 31) sw[warp_id()] = incl;
+      __syncthreads();
+      int wbase = 0;
+      for (int w = 0; w < warp_id(); ++w) wbase += sw[w];
+      const int start = wbase + incl - (c0 + c1);
+      __syncthreads();
+      hist[b0] = start;  // becomes the bin's write cursor
+      hist[b1] = start + c0;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < L; s += kHriThreads) {
+      const int u = g.adj[o + s];
+      if (u < 0) continue;
+      const int c = g.color[u] & kColorMask;
+      const int pos = atomicAdd(&hist[hri_bin(c)], 1);
+      if (pos < room)
+        h.pairs[base + pos] = ((unsigned long long)(unsigned)c << 32) | (unsigned)u;
+      else
+        atomicOr(&st->status, ST_OVERFLOW);
+    }
+    __syncthreads();
+  }
+}
+
+static_assert(kHriBins == 2 * kHriThreads, "fill scan: two bins per thread");
+
+}  // namespace
+
+cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, cudaStream_t s) {
+  if (h.min_live <= 0 || g.n <= 0) return cudaSuccess;
+  long long b = ((long long)g.n + kHriThreads - 1) / kHriThreads;
+  if (b > 148 * 16) b = 148 * 16;
+  hri_classify_kernel<<<(unsigned)b, kHriThreads, 0, s>>>(g, h, st);
+  hri_offsets_kernel<<<1, kHriThreads, 0, s>>>(g, h, st);
+  hri_fill_kernel<<<148 * 4, kHriThreads, 0, s>>>(g, h, st);
+  return cudaGetLastError();
+}
+
+}  // namespace dc

@@ -81,6 +81,12 @@ struct DevState {
   unsigned long long t_struct[2];     // %globaltimer at the start and end of the structural launch
   unsigned long long t_recolor[2];    // same for the recolour launch
   unsigned long long phase_ns[6];     // recolour launch: seeding, find-eligible, mex, commit, 2 spare
+  // heavy-row index (HI)
+  unsigned long long hcount;          // rows found with at least min_live live slots
+  unsigned long long a_count;         // (vertex, chunk) items waiting for the append phase
+  unsigned hri_off;                   // 1: the index is incomplete for this batch; full scans only
+  unsigned pad1;
+  long long read_delta;               // adjacency/index entries read minus entries scanned
 };
 
 struct GraphDev {
@@ -139,6 +145,30 @@ struct StructParams {
   DevState* st;
 };
 
+// Heavy-row index (HI only).  Per batch, every row with at least
+// `min_live` live slots gets a copy of its neighbours ordered by their colour
+// at the start of the recolour launch (descending), and a list of its
+// neighbours whose colour has changed since.  findEligibleNeighbors marks a
+// neighbour u of v only if color[u] > prev[v] or color[u] == color[v], so
+// for such a row it reads the head of the ordered copy, the segment of
+// colour color[v], and the list, instead of gathering every neighbour's
+// colour.
+constexpr int kHeavyMinLive = 2048;
+constexpr int kHriBins = 1024;  // exact colour order below 1023; colours >= 1023 share the first bin
+struct HriBufs {
+  int* hid;                   // n: index of v's ordered copy, or -1
+  int* hrow;                  // cap_rows: vertex of index i
+  long long* hoff;            // cap_rows + 1: start of row i in pairs
+  unsigned long long* pairs;  // cap_pairs: (colour << 32) | neighbour
+  long long* xoff;            // cap_rows + 1: start of row i's change list
+  int* xcnt;                  // cap_rows: entries appended to row i's change list (> capacity: overflow)
+  int* xv;                    // cap_exc: changed neighbours
+  unsigned* bmF;              // n/32 + 1: colour changed since the index was built
+  int2* alist;                // cap_a: (vertex, chunk) of first changes, for the append phase
+  long long cap_rows, cap_pairs, cap_exc, cap_a;
+  int min_live;               // 0: no index
+};
+
 struct RecolorParams {
   GraphDev g;
   const dc_change* ch;
@@ -154,6 +184,7 @@ struct RecolorParams {
   int* ncolor;           // n
   int* sat;              // n
   unsigned long long* cp;  // HB: n packed (degree property, colour) words
+  HriBufs hri;             // HI: heavy-row index (hri.min_live == 0: off)
   unsigned char* lflag;  // k
   // Batched mode: the graph is a disjoint union of independent graphs.
   const int* gid;        // vertex -> graph (nullptr: one graph)
@@ -193,5 +224,7 @@ cudaError_t launch_range_gather(const GraphDev& g, int base, int v0, int nv, con
 cudaError_t launch_range_scatter(const GraphDev& g, int base, int v0, int nv, const long long* pre, const int* in,
                                  cudaStream_t s);
 cudaError_t launch_fill(int* p, long long count, int value, cudaStream_t s);
+// Builds the heavy-row index of the current graph and colours (dc_hri.cu).
+cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, cudaStream_t s);
 
 }  // namespace dc

@@ -141,6 +141,10 @@ struct Env {
   // HB: (degree property << 32) | colour word per vertex, so one 8-byte
   // gather gives both; the next-frontier mark lives in its colour half
   unsigned long long* cp;
+  // HI: heavy-row index (hri_on false: every row is scanned in full)
+  HriBufs hri;
+  bool hri_on;
+  long long read_delta;  // entries read minus entries the rules cover
   // batched mode (all nullptr for one graph)
   const int* gid;
   int* gpush;        // HI: pushes into the next frontier per graph, this iteration
@@ -451,6 +455,123 @@ __device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, 
   if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
 }
 
+// HI findEligibleNeighbors over one unit of an indexed row v: the unit's
+// slice of the colour-ordered copy (candidates are the neighbours whose
+// colour at index time is above prev[v], equal to color[v], or in the shared
+// top bin; a slice that starts below both is skipped after one load), then
+// the same slice of v's change list.  Every candidate's current colour is
+// gathered and the reference's rule applied to it.
+__device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi, long long xb, int xc,
+                             const QueueBufs& nq, QCount* nc) {
+  const HriBufs& H = E.hri;
+  const long long p0 = H.hoff[hi] + (long long)un.y * E.CH;
+  const long long p1 = min(H.hoff[hi + 1], p0 + E.CH);
+  long long reads = 0;
+  if (p0 < p1) {
+    const int sf = (int)(H.pairs[p0] >> 32);
+    const bool skip = sf < kHriBins - 1 && sf <= R.pv && sf < R.cv;
+    reads = 1;
+    if (lane_id() == 0) E.my_scanned += p1 - p0;  // the rule covers every live entry
+    if (!skip) {
+      for (long long r0 = p0; r0 < p1; r0 += 128) {
+        reads = min(p1, r0 + 128) - p0;
+        int uu[4];
+        unsigned ww[4];
+        bool mu[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const long long idx = r0 + j * 32 + lane_id();
+          uu[j] = -1;
+          if (idx < p1) {
+            const unsigned long long x = H.pairs[idx];
+            const int c0 = (int)(x >> 32);
+            if (c0 >= kHriBins - 1 || c0 > R.pv || c0 == R.cv) uu[j] = (int)(unsigned)x;
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) ww[j] = uu[j] >= 0 ? (unsigned)E.g.color[uu[j]] : kMarkBit;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int cu = (int)(ww[j] & (unsigned)kColorMask);
+          mu[j] = uu[j] >= 0 && ((R.cv == cu && R.v < uu[j]) || (R.pv < cu));
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
+        // the copy is in descending colour order: once a round ends below
+        // both thresholds, so does the rest of the slice
+        const int sl = (int)(H.pairs[min(r0 + 127, p1 - 1)] >> 32);
+        if (sl < kHriBins - 1 && sl <= R.pv && sl < R.cv) break;
+      }
+    }
+  }
+  const long long e0 = (long long)un.y * E.CH;
+  const long long e1 = min((long long)xc, e0 + E.CH);
+  if (e0 < e1) {
+    reads += e1 - e0;
+    for (long long r0 = e0; r0 < e1; r0 += 128) {
+      int uu[4];
+      unsigned ww[4];
+      bool mu[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const long long idx = r0 + j * 32 + lane_id();
+        uu[j] = idx < e1 ? H.xv[xb + idx] : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) ww[j] = uu[j] >= 0 ? (unsigned)E.g.color[uu[j]] : kMarkBit;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int cu = (int)(ww[j] & (unsigned)kColorMask);
+        mu[j] = uu[j] >= 0 && ((R.cv == cu && R.v < uu[j]) || (R.pv < cu));
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
+    }
+  }
+  if (lane_id() == 0) E.read_delta += reads - (p1 > p0 ? p1 - p0 : 0);
+}
+
+// First colour change of v since the index was built: queue v's row, in
+// chunks, for the append phase.  An overflowing queue turns the index off
+// for the rest of the batch.
+__device__ __forceinline__ void push_first(Env& E, int v) {
+  const int L = E.g.len[v];
+  const int c = L > 0 ? (L + E.CH - 1) / E.CH : 0;
+  if (c == 0) return;
+  const unsigned long long b = atomicAdd(&E.st->a_count, (unsigned long long)c);
+  if ((long long)(b + c) > E.hri.cap_a) {
+    atomicExch(&E.st->hri_off, 1u);
+    return;
+  }
+  for (int q = 0; q < c; ++q) E.hri.alist[b + q] = make_int2(v, q);
+}
+
+// Append phase: every vertex whose colour changed for the first time since
+// the index was built joins the change list of each indexed neighbour.
+__device__ void phase_append(Env& E, unsigned long long* ctr) {
+  const HriBufs& H = E.hri;
+  // an overflowed queue has unwritten items, and the index is off anyway
+  if (ld_cg(&E.st->hri_off) != 0u) return;
+  const long long cnt = min((long long)ld_cg(&E.st->a_count), H.cap_a);
+  while (true) {
+    const long long i = grab(ctr);
+    if (i >= cnt) break;
+    const int2 it = H.alist[i];
+    const int v = it.x;
+    const int L = E.g.len[v];
+    const long long o = E.g.off[v];
+    const int s_lo = it.y * E.CH, s_hi = min(L, s_lo + E.CH);
+    for (int s = s_lo + lane_id(); s < s_hi; s += 32) {
+      const int u = E.g.adj[o + s];
+      if (u < 0) continue;
+      const int h = H.hid[u];
+      if (h < 0) continue;
+      const int slot = atomicAdd(&H.xcnt[h], 1);
+      if ((long long)slot < H.xoff[h + 1] - H.xoff[h]) H.xv[H.xoff[h] + slot] = v;
+    }
+  }
+}
+
 __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, QCount* nc) {
   const GraphDev& g = E.g;
   const int v = un.x;
@@ -463,6 +584,17 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
   R.v = v;
   R.cv = g.color[v] & kColorMask;
   R.pv = E.variant == DC_HI ? g.prev[v] : g.prop[v];
+  if (E.hri_on) {
+    const int hi = E.hri.hid[v];
+    if (hi >= 0 && ld_cg(&E.st->hri_off) == 0u) {
+      const long long xb = E.hri.xoff[hi];
+      const int xc = ld_cg(&E.hri.xcnt[hi]);
+      if ((long long)xc <= E.hri.xoff[hi + 1] - xb) {  // its change list is complete
+        expand_heavy(E, pb, un, R, hi, xb, xc, nq, nc);
+        return;
+      }
+    }
+  }
   bool markv = false;
   int nx[4];  // ids of the next round, loaded one round ahead
 #pragma unroll
@@ -621,6 +753,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
   for (long long i0 = gwarp * 32; i0 < total; i0 += nwarps * 32) {
     const int v = queue_item(qb, cA, total, i0 + lane_id());
     int push = -1;
+    int first = -1;  // first colour change since the heavy-row index was built
     if (v >= 0) {
       ++items;
       switch (kind) {
@@ -631,6 +764,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           if (nc != oc) {
             changed = true;
             if (E.gchg) atomicAdd(&E.gchg[E.gid[v]], 1);
+            if (E.hri_on && mark_bit(E.hri.bmF, v)) first = v;
           }
           g.color[v] = nc;  // also clears the frontier mark
           if (E.cp) reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)nc;
@@ -642,6 +776,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           const int nc = ld_cg(&E.p.ncolor[v]);
           const int oc = g.color[v];
           if (nc != oc) {
+            if (E.hri_on && mark_bit(E.hri.bmF, v)) first = v;
             if (kind == C_SEED_DEL) g.prev[v] = oc;
             g.color[v] = nc;
             if (E.cp) reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)nc;
@@ -653,6 +788,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
         }
         case C_SEED_INS: {
           const int nc = ld_cg(&E.p.ncolor[v]);
+          if (E.hri_on && nc != g.color[v] && mark_bit(E.hri.bmF, v)) first = v;
           g.prev[v] = g.color[v];
           g.color[v] = nc;
           cmax_local = max(cmax_local, nc);
@@ -668,6 +804,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           break;
       }
     }
+    if (first >= 0) push_first(E, first);
     if (f0) {
       const bool claim = push >= 0 && mark_bit(E.p.bmB, push);
       if (claim && E.gf0) atomicAdd(&E.gf0[E.gid[push]], 1);
@@ -704,6 +841,9 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.gskip = nullptr;
   E.gf0 = p.gid ? p.gf0 : nullptr;
   E.cp = V == DC_HB ? p.cp : nullptr;
+  E.hri = p.hri;
+  E.hri_on = V == DC_HI && p.hri.min_live > 0;
+  E.read_delta = 0;
   DevState* st = p.st;
   const GraphDev& g = E.g;
   unsigned bar = 0;
@@ -845,6 +985,13 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     for (long long gg = gtid; gg < p.ngraphs; gg += gthreads) p.gstate[gg] = ld_cg(&p.gf0[gg]) > 0 ? 1 : 2;
   }
   if (!grid_sync(st, bar)) return;
+  // rows of vertices the seeding recoloured join their indexed neighbours'
+  // change lists before the loop reads them
+  if (E.hri_on && ld_cg(&st->a_count) > 0) {
+    phase_append(E, ctr());
+    ++ps;
+    if (!grid_sync(st, bar)) return;
+  }
   lap(0);
 
   // ======================= loop =======================
@@ -869,6 +1016,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         z->countA = 0;
         z->countU = 0;
         z->masks = 0;
+        st->a_count = 0;  // every warp read it before the append phase's barrier
       }
       const int ring = (int)(it & 1);
       if (p.gid) {
@@ -921,6 +1069,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       phase_commit(E, p.qb[nb], nc, C_LOOP, nullptr, nullptr, gwarp, nwarps, &st->frontier_total,
                    &st->chg[it & 1]);
       if (!grid_sync(st, bar)) return;
+      if (E.hri_on && ld_cg(&st->a_count) > 0) {
+        phase_append(E, ctr());
+        ++ps;
+        if (!grid_sync(st, bar)) return;
+      }
       lap(3);
       if (V == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;
       fs = ns;
@@ -938,9 +1091,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     }
   }
   const long long sc = warp_sum_ll(E.my_scanned);
+  const long long rd = warp_sum_ll(E.read_delta);
   if (lane_id() == 0 && sc) {
     atomicAdd(&st->slots_scanned, (unsigned long long)sc);
-    atomicAdd(&st->slots_read, (unsigned long long)sc);  // every scan reads its row once
+    atomicAdd(&st->slots_read, (unsigned long long)(sc + rd));  // entries actually read
   }
 }
 

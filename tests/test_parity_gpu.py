@@ -308,3 +308,30 @@ def test_greedy_initial_colouring_of_the_resident_graph():
     assert np.array_equal(ctx.colors(), dc.greedy_color(n, x[keep], y[keep]))
     assert ctx.validate() == 0
     ctx.close()
+
+
+@pytest.mark.parametrize("min_live,unit_slots", [(64, 128), (256, 2048), (-1, 2048)])
+def test_heavy_row_index_matches_oracle(min_live, unit_slots):
+    """HI with the per-batch colour index of heavy rows (many rows indexed,
+    rows split over many units, and the index off): colours, iterations,
+    frontier sizes and covered entries stay those of the oracle, while the
+    entries actually read drop when the index is on."""
+    n, a, b = rmat_graph(14, 16, seed=5)
+    col = dc.greedy_color(n, a, b)
+    es = dc.EdgeSet(n, a, b)
+    ctx = gpu_ctx(dc.HI, n, a, b, col, unit_slots=unit_slots, heavy_min_live=min_live)
+    g = oracle_graph(n, a, b, col)
+    read = scanned = 0
+    for i in range(4):
+        ch = es.sample_batch(4000, 4000, mode=dc.INS_RMAT, scale=14, seed=40 + i)
+        rc, so = g.apply_batch(ch, po.HI, po.SNAPSHOT)
+        sg = ctx.apply_batch(to_dc_changes(ch))
+        check_same(ctx, g, sg, so)
+        read += sg.slots_read
+        scanned += sg.slots_scanned
+    assert ctx.validate() == 0
+    if min_live > 0:
+        assert read < scanned
+    else:
+        assert read == scanned
+    ctx.close()
