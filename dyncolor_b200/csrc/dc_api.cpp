@@ -83,6 +83,8 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     if ((s = dalloc(ctx, &h.pairs, h.cap_pairs, "ordered neighbours")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.xv, h.cap_exc, "change lists")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.alist, h.cap_a, "append queue")) != DC_OK) return s;
+    h.cap_hist = std::min<long long>(h.cap_rows, 1ll << 16);
+    if ((s = dalloc(ctx, &h.hist, h.cap_hist * kHriBins, "heavy-row colour counts")) != DC_OK) return s;
   }
   if (!ctx->bmA) {
     if ((s = dalloc(ctx, &ctx->bmA, words, "bitmap")) != DC_OK) return s;
@@ -650,6 +652,7 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->hri.pairs);
   dfree(ctx, &ctx->hri.xv);
   dfree(ctx, &ctx->hri.alist);
+  dfree(ctx, &ctx->hri.hist);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->len);
   dfree(ctx, &ctx->cap);

@@ -9,7 +9,8 @@
 //             buffers' capacity lose their index and are scanned in full
 //   fill      one CTA per row: counting sort of the row's live neighbours
 //             by colour, descending (colours >= kHriBins - 1 share the first
-//             bin), written as (colour << 32) | neighbour
+//             bin), written as (colour << 32) | neighbour; the first
+//             cap_hist rows also keep their per-colour counts
 #include "dc_device.cuh"
 
 namespace dc {
@@ -107,6 +108,9 @@ __global__ void __launch_bounds__(kHriThreads) hri_fill_kernel(GraphDev g, HriBu
       if (u >= 0) atomicAdd(&hist[hri_bin(g.color[u] & kColorMask)], 1);
     }
     __syncthreads();
+    // the mex of the loop reads the per-colour counts of the first cap_hist rows
+    if (i < h.cap_hist)
+      for (int b = threadIdx.x; b < kHriBins; b += kHriThreads) h.hist[i * kHriBins + b] = hist[b];
     // descending bins: start of bin b = sum of the counts of bins above b.
     // Thread t owns bins [2t, 2t + 1] counted from the top.
     {

@@ -165,7 +165,8 @@ struct HriBufs {
   int* xv;                    // cap_exc: changed neighbours
   unsigned* bmF;              // n/32 + 1: colour changed since the index was built
   int2* alist;                // cap_a: (vertex, chunk) of first changes, for the append phase
-  long long cap_rows, cap_pairs, cap_exc, cap_a;
+  int* hist;                  // cap_hist * kHriBins: row i's neighbour count per colour at build time
+  long long cap_rows, cap_pairs, cap_exc, cap_a, cap_hist;
   int min_live;               // 0: no index
 };
 

@@ -144,6 +144,7 @@ struct Env {
   // HI: heavy-row index (hri_on false: every row is scanned in full)
   HriBufs hri;
   bool hri_on;
+  bool hri_mex;          // the loop's mex may use the index (its change lists are complete)
   long long read_delta;  // entries read minus entries the rules cover
   // batched mode (all nullptr for one graph)
   const int* gid;
@@ -156,12 +157,12 @@ struct Env {
 // ---------------------------------------------------------------------
 // slow paths (single warp, whole row): colour windows beyond the first
 // ---------------------------------------------------------------------
-__device__ int slow_mex(Env& E, unsigned* sm, int v, int mode) {
+__device__ int slow_mex(Env& E, unsigned* sm, int v, int mode, int w_first = kMaskBits) {
   const GraphDev& g = E.g;
   const long long o = g.off[v];
   const int L = g.len[v];
   const int pv = mode == M_MEX_PRIOR ? g.prop[v] : 0;
-  for (int w0 = kMaskBits;; w0 += kMaskBits) {
+  for (int w0 = w_first;; w0 += kMaskBits) {
     for (int k = lane_id(); k < kMaskWords; k += 32) sm[k] = 0;
     __syncwarp();
     for (int s0 = 0; s0 < L; s0 += 32) {
@@ -224,7 +225,72 @@ __device__ __forceinline__ void fold_low(unsigned* sm, unsigned long long lm) {
   __syncwarp();
 }
 
+// HI mex of an indexed row v inside the loop, from the index instead of a
+// gather per neighbour: colour c is present iff some neighbour that kept
+// its launch-start colour has colour c (the row's colour-c segment of the
+// ordered copy holds a vertex not marked as changed), or some changed
+// neighbour has colour c now (its change list).  Colours are tried in
+// increasing order 32 at a time.  Returns false when the row has no usable
+// index (the caller scans it); the whole row is handled by its first unit.
+__device__ bool reduce_heavy(Env& E, Shared& sh, int4 un, int* out) {
+  const HriBufs& H = E.hri;
+  const int v = un.x;
+  const int hi = H.hid[v];
+  if (hi < 0 || hi >= H.cap_hist || ld_cg(&E.st->hri_off) != 0u) return false;
+  const long long xb = H.xoff[hi];
+  const int xc = ld_cg(&H.xcnt[hi]);
+  if ((long long)xc > H.xoff[hi + 1] - xb) return false;  // change list overflowed
+  if (un.y != 0) return true;
+  const long long pe = H.hoff[hi + 1];
+  if (lane_id() == 0) E.my_scanned += pe - H.hoff[hi];  // the rule covers every live entry
+  unsigned* sm = sh.mask[warp_id()];
+  for (int k = lane_id(); k < kMaskWords; k += 32) sm[k] = 0;
+  __syncwarp();
+  for (int j = lane_id(); j < xc; j += 32) {
+    const int u = H.xv[xb + j];
+    const int c = E.g.color[u] & kColorMask;
+    if (c < kMaskBits) atomicOr(&sm[c >> 5], 1u << (c & 31));
+  }
+  __syncwarp();
+  const int* hist = H.hist + (long long)hi * kHriBins;
+  long long below = 0;  // neighbours (at launch start) with a colour below the chunk
+  long long reads = xc;
+  int r = -1;
+  for (int c0 = 0; c0 < kHriBins - 1; c0 += 32) {
+    const int c = c0 + lane_id();
+    const int cnt = c < kHriBins - 1 ? hist[c] : 0;
+    const int incl = warp_incl_scan(cnt);
+    // colour c's segment: the copy is descending, so it ends where the
+    // colours below c begin
+    const long long seg_end = pe - (below + incl - cnt);
+    bool pres = c >= kHriBins - 1 || ((sm[c >> 5] >> (c & 31)) & 1u);
+    for (int q = 1; !pres && q <= cnt; ++q) {
+      const int u = (int)(unsigned)H.pairs[seg_end - q];
+      ++reads;
+      pres = !((ld_cg(&H.bmF[u >> 5]) >> (u & 31)) & 1u);
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, pres);
+    below += __shfl_sync(0xffffffffu, incl, 31);
+    if (bal != 0xffffffffu) {
+      r = c0 + __ffs(~bal) - 1;
+      break;
+    }
+  }
+  if (r < 0) {
+    // every colour below the shared top bin is present: scan the row
+    reads += pe - H.hoff[hi];
+    r = slow_mex(E, sm, v, M_MEX_ALL, 0);
+  }
+  if (lane_id() == 0) {
+    out[v] = r;
+    E.read_delta += reads - (pe - H.hoff[hi]);
+  }
+  __syncwarp();
+  return true;
+}
+
 __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, int mode, int* out) {
+  if (E.hri_mex && mode == M_MEX_ALL && reduce_heavy(E, sh, un, out)) return;
   const GraphDev& g = E.g;
   const int v = un.x, chunk = un.y, ms = un.z, nch = un.w;
   const int L = g.len[v];
@@ -843,6 +909,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.cp = V == DC_HB ? p.cp : nullptr;
   E.hri = p.hri;
   E.hri_on = V == DC_HI && p.hri.min_live > 0;
+  E.hri_mex = false;  // set once the seeding's changes are in the change lists
   E.read_delta = 0;
   DevState* st = p.st;
   const GraphDev& g = E.g;
@@ -992,6 +1059,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     ++ps;
     if (!grid_sync(st, bar)) return;
   }
+  E.hri_mex = E.hri_on;
   lap(0);
 
   // ======================= loop =======================
