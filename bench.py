@@ -62,6 +62,8 @@ def parse_args():
                     help="reference arm: a step's loop stops once its timed work passes this budget")
     ap.add_argument("--unit-slots", type=int, default=0, help="adjacency slots per warp work unit (0: library default)")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent CTAs per SM (0: from occupancy)")
+    ap.add_argument("--heavy-min-live", type=int, default=0,
+                    help="HI: live slots from which a row is indexed by colour (0: library default, <0: off)")
     ap.add_argument("--mode", choices=["plain", "batched", "served"], default="plain",
                     help="plain: one large graph (headline); batched: many graphs in one launch; "
                          "served: request stream over resident graphs")
@@ -371,7 +373,7 @@ def run_ours(args, dist: Dist):
     variant = dc.HI if args.variant == "hi" else dc.HB
     stream = torch.cuda.Stream(device=dev)
     ctx = dc.Context(variant=variant, device=dev, stream=stream.cuda_stream, unit_slots=args.unit_slots,
-                     blocks_per_sm=args.blocks_per_sm)
+                     blocks_per_sm=args.blocks_per_sm, heavy_min_live=args.heavy_min_live)
     t0 = time.time()
     ctx.load_edges(w["n"], w["a"], w["b"])
     ctx.set_colors(w["colors"])
