@@ -75,7 +75,7 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     h.cap_rows = ctx->pool_cap / h.min_live + 1;
     h.cap_pairs = ctx->pool_cap / 8 + 4096;
     h.cap_exc = h.cap_pairs / 4 + 64 * h.cap_rows;
-    h.cap_a = n / 8 + ctx->pool_cap / CH + 1024;
+    h.cap_a = n / 8 + ctx->pool_cap / 512 + 1024;  // items of 512 slots
     if ((s = dalloc(ctx, &h.hrow, h.cap_rows, "heavy rows")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.hoff, h.cap_rows + 1, "heavy-row offsets")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.xoff, h.cap_rows + 1, "change-list offsets")) != DC_OK) return s;

@@ -600,9 +600,11 @@ __device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi
 // First colour change of v since the index was built: queue v's row, in
 // chunks, for the append phase.  An overflowing queue turns the index off
 // for the rest of the batch.
+constexpr int kAppendChunk = 512;  // slots per append-phase item: 4 rounds of 4 loads per lane
+
 __device__ __forceinline__ void push_first(Env& E, int v) {
   const int L = E.g.len[v];
-  const int c = L > 0 ? (L + E.CH - 1) / E.CH : 0;
+  const int c = L > 0 ? (L + kAppendChunk - 1) / kAppendChunk : 0;
   if (c == 0) return;
   const unsigned long long b = atomicAdd(&E.st->a_count, (unsigned long long)c);
   if ((long long)(b + c) > E.hri.cap_a) {
@@ -626,14 +628,23 @@ __device__ void phase_append(Env& E, unsigned long long* ctr) {
     const int v = it.x;
     const int L = E.g.len[v];
     const long long o = E.g.off[v];
-    const int s_lo = it.y * E.CH, s_hi = min(L, s_lo + E.CH);
-    for (int s = s_lo + lane_id(); s < s_hi; s += 32) {
-      const int u = E.g.adj[o + s];
-      if (u < 0) continue;
-      const int h = H.hid[u];
-      if (h < 0) continue;
-      const int slot = atomicAdd(&H.xcnt[h], 1);
-      if ((long long)slot < H.xoff[h + 1] - H.xoff[h]) H.xv[H.xoff[h] + slot] = v;
+    const int s_lo = it.y * kAppendChunk, s_hi = min(L, s_lo + kAppendChunk);
+    for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
+      int uu[4], hh[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int sidx = r0 + j * 32 + lane_id();
+        uu[j] = sidx < s_hi ? E.g.adj[o + sidx] : -1;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) hh[j] = uu[j] >= 0 ? H.hid[uu[j]] : -1;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (hh[j] < 0) continue;
+        const int h = hh[j];
+        const int slot = atomicAdd(&H.xcnt[h], 1);
+        if ((long long)slot < H.xoff[h + 1] - H.xoff[h]) H.xv[H.xoff[h] + slot] = v;
+      }
     }
   }
 }
