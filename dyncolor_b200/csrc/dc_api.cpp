@@ -73,8 +73,8 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     HriBufs& h = ctx->hri;
     h.min_live = ctx->opt.heavy_min_live;
     h.cap_rows = ctx->pool_cap / h.min_live + 1;
-    h.cap_pairs = ctx->pool_cap / 8 + 4096;
-    h.cap_exc = h.cap_pairs / 4 + 64 * h.cap_rows;
+    h.cap_pairs = ctx->pool_cap / 4 + 4096;  // R-MAT scale 24: rows >= 2048 hold 236 M of 1.57 G slots
+    h.cap_exc = h.cap_pairs;  // a row's change list holds at most its live neighbours
     h.cap_a = n / 8 + ctx->pool_cap / 512 + 1024;  // items of 512 slots
     if ((s = dalloc(ctx, &h.hrow, h.cap_rows, "heavy rows")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.hoff, h.cap_rows + 1, "heavy-row offsets")) != DC_OK) return s;

@@ -21,8 +21,9 @@ constexpr int kHriThreads = 512;
 
 __device__ __forceinline__ int hri_bin(int c) { return c < kHriBins - 1 ? c : kHriBins - 1; }
 
-// Change-list capacity of a row with `live` slots.
-__device__ __forceinline__ long long xcap(int live) { return live / 4 + 64; }
+// Change-list capacity of a row with `live` slots: a neighbour joins the
+// list once per launch (at its first colour change), so it never overflows.
+__device__ __forceinline__ long long xcap(int live) { return live; }
 
 __global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
   const long long nt = (long long)gridDim.x * blockDim.x;
