@@ -274,7 +274,7 @@ def hbm_peak():
 # launch, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum,
 # one pass) of this bench's own default workload: R-MAT scale 24, 1 M-line
 # batches, HI: 916.3 GB for 168.5 G entries.
-MEASURED_DRAM_BYTES_PER_ENTRY = {("hi", 24, 16, 1_000_000): 5.44}
+MEASURED_DRAM_BYTES_PER_ENTRY = {}
 
 
 def load_traffic(args):
@@ -458,6 +458,8 @@ def run_ours(args, dist: Dist):
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg / K,
+                     "entries_covered_per_launch": scanned / K,
+                     "entries_read_per_launch": sum(s.slots_read for s in stats) / K,
                      "note": f"{per_slot} B per scanned adjacency entry (id + neighbour colour"
                              + (" + priority" if variant == dc.HB else "") + ")"},
         "clocks": clk,
