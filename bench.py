@@ -270,11 +270,12 @@ def hbm_peak():
         return HBM_FALLBACK_GBS, "fallback"
 
 
-# DRAM bytes (read + write) per scanned adjacency entry of the recolour
+# DRAM bytes (read + write) per covered adjacency entry of the recolour
 # launch, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum,
 # one pass) of this bench's own default workload: R-MAT scale 24, 1 M-line
-# batches, HI: 916.3 GB for 168.5 G entries.
-MEASURED_DRAM_BYTES_PER_ENTRY = {}
+# batches, HI, heavy-row index on: 302.6 GB for 168.5 G covered entries
+# (32.1 G of them actually read).
+MEASURED_DRAM_BYTES_PER_ENTRY = {("hi", 24, 16, 1_000_000): 1.80}
 
 
 def load_traffic(args):
