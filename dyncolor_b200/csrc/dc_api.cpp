@@ -68,23 +68,27 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     q.capU = capU;
     q.capM = capM;
   }
-  if (ctx->opt.variant == DC_HI && ctx->opt.heavy_min_live > 0) {
+  if (ctx->opt.heavy_min_live > 0) {
     // heavy-row index: rows that do not fit lose their index (and are scanned in full)
+    const bool hi = ctx->opt.variant == DC_HI;
     HriBufs& h = ctx->hri;
     h.min_live = ctx->opt.heavy_min_live;
     h.cap_rows = ctx->pool_cap / h.min_live + 1;
     h.cap_pairs = ctx->pool_cap / 4 + 4096;  // R-MAT scale 24: rows >= 2048 hold 236 M of 1.57 G slots
-    h.cap_exc = h.cap_pairs;  // a row's change list holds at most its live neighbours
-    h.cap_a = n / 8 + ctx->pool_cap / 512 + 1024;  // items of 512 slots
+    h.cap_exc = hi ? h.cap_pairs : 1;       // a row's change list holds at most its live neighbours
+    h.cap_a = hi ? n / 8 + ctx->pool_cap / 512 + 1024 : 1;  // items of 512 slots
+    h.cap_hist = hi ? std::min<long long>(h.cap_rows, 1ll << 16) : 0;
     if ((s = dalloc(ctx, &h.hrow, h.cap_rows, "heavy rows")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.hoff, h.cap_rows + 1, "heavy-row offsets")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.xoff, h.cap_rows + 1, "change-list offsets")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.xcnt, h.cap_rows, "change-list counts")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.hsplit, h.cap_rows, "priority splits")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.pairs, h.cap_pairs, "ordered neighbours")) != DC_OK) return s;
-    if ((s = dalloc(ctx, &h.xv, h.cap_exc, "change lists")) != DC_OK) return s;
-    if ((s = dalloc(ctx, &h.alist, h.cap_a, "append queue")) != DC_OK) return s;
-    h.cap_hist = std::min<long long>(h.cap_rows, 1ll << 16);
-    if ((s = dalloc(ctx, &h.hist, h.cap_hist * kHriBins, "heavy-row colour counts")) != DC_OK) return s;
+    if (hi) {
+      if ((s = dalloc(ctx, &h.xv, h.cap_exc, "change lists")) != DC_OK) return s;
+      if ((s = dalloc(ctx, &h.alist, h.cap_a, "append queue")) != DC_OK) return s;
+      if ((s = dalloc(ctx, &h.hist, h.cap_hist * kHriBins, "heavy-row colour counts")) != DC_OK) return s;
+    }
   }
   if (!ctx->bmA) {
     if ((s = dalloc(ctx, &ctx->bmA, words, "bitmap")) != DC_OK) return s;
@@ -93,10 +97,11 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     if ((s = dalloc(ctx, &ctx->ncolor, n, "ncolor")) != DC_OK) return s;
     if ((s = dalloc(ctx, &ctx->sat, n, "sat")) != DC_OK) return s;
     if (ctx->opt.variant == DC_HB && (s = dalloc(ctx, &ctx->cp, n, "packed words")) != DC_OK) return s;
-    if (ctx->opt.variant == DC_HI && ctx->opt.heavy_min_live > 0) {
+    if (ctx->opt.heavy_min_live > 0) {
       HriBufs& h = ctx->hri;
       if ((s = dalloc(ctx, &h.hid, n, "heavy-row ids")) != DC_OK) return s;
-      if ((s = dalloc(ctx, &h.bmF, words, "changed-colour bitmap")) != DC_OK) return s;
+      if (ctx->opt.variant == DC_HI && (s = dalloc(ctx, &h.bmF, words, "changed-colour bitmap")) != DC_OK)
+        return s;
     }
     DC_CK(cudaMemsetAsync(ctx->bmA, 0, words * 4, ctx->stream));
     DC_CK(cudaMemsetAsync(ctx->bmB, 0, words * 4, ctx->stream));
@@ -394,7 +399,8 @@ dc_status enqueue_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const
     const size_t b0 = offsetof(DevState, bar_arrived);
     const size_t b1 = offsetof(DevState, wctr) + sizeof(((DevState*)nullptr)->wctr);
     DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
-    if (ctx->hri.min_live > 0) DC_CK(launch_hri_build(graph_dev(ctx), ctx->hri, ctx->st, ctx->stream));
+    if (ctx->hri.min_live > 0)
+      DC_CK(launch_hri_build(graph_dev(ctx), ctx->hri, ctx->st, ctx->opt.variant, ctx->stream));
     RecolorParams rp = recolor_params(ctx, d_ch, k);
     rp.k_dev = k_dev;
     DC_CK(launch_recolor(rp, ctx->grid_recolor, ctx->stream));
@@ -580,7 +586,7 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   if (o.unit_slots <= 0) o.unit_slots = kUnitSlotsDefault;
   if (o.unit_slots % 128 != 0 || o.unit_slots < 128) return DC_E_INVAL;
   if (o.heavy_min_live == 0) o.heavy_min_live = kHeavyMinLive;
-  if (o.heavy_min_live < 0 || o.variant != DC_HI) o.heavy_min_live = 0;  // off
+  if (o.heavy_min_live < 0) o.heavy_min_live = 0;  // off
   if (o.heavy_min_live > 0 && o.heavy_min_live < 64) o.heavy_min_live = 64;
   dc_ctx* ctx = new (std::nothrow) dc_ctx();
   if (!ctx) return DC_E_NOMEM;
@@ -653,6 +659,7 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->hri.xv);
   dfree(ctx, &ctx->hri.alist);
   dfree(ctx, &ctx->hri.hist);
+  dfree(ctx, &ctx->hri.hsplit);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->len);
   dfree(ctx, &ctx->cap);

@@ -1,4 +1,4 @@
-// dc_hri.cu -- heavy-row index of the HI recolouring loop, rebuilt before
+// dc_hri.cu -- heavy-row index of the recolouring loop, rebuilt before
 // every recolour launch (after the structural update of the batch).
 //
 //   classify  rows with at least min_live live slots get an index i (in
@@ -7,10 +7,12 @@
 //   offsets   one CTA: exclusive scans of the rows' live counts (ordered
 //             copies) and of their change-list capacities; rows past the
 //             buffers' capacity lose their index and are scanned in full
-//   fill      one CTA per row: counting sort of the row's live neighbours
+//   fill (HI) one CTA per row: counting sort of the row's live neighbours
 //             by colour, descending (colours >= kHriBins - 1 share the first
 //             bin), written as (colour << 32) | neighbour; the first
 //             cap_hist rows also keep their per-colour counts
+//   split (HB) one CTA per row: the neighbours prior to the row's vertex in
+//             LDF order first, then the rest
 #include "dc_device.cuh"
 
 namespace dc {
@@ -39,8 +41,10 @@ __global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
     }
     h.hid[v] = id;
   }
-  const long long words = ((long long)g.n + 31) / 32 + 1;
-  for (long long w = t; w < words; w += nt) h.bmF[w] = 0u;
+  if (h.bmF) {
+    const long long words = ((long long)g.n + 31) / 32 + 1;
+    for (long long w = t; w < words; w += nt) h.bmF[w] = 0u;
+  }
 }
 
 // Single CTA.  hoff / xoff get exclusive prefixes; rows whose copy or list
@@ -148,15 +152,62 @@ __global__ void __launch_bounds__(kHriThreads) hri_fill_kernel(GraphDev g, HriBu
 
 static_assert(kHriBins == 2 * kHriThreads, "fill scan: two bins per thread");
 
+// HB: one CTA per row: the row's live neighbours prior to v in LDF order
+// (HB/gpuFunctions_undir.cuh:104-113) first, then the others.  The
+// prior-filtered mex of v only needs the first part.
+__global__ void __launch_bounds__(kHriThreads) hri_split_kernel(GraphDev g, HriBufs h, DevState* st) {
+  __shared__ int s_cur[2];
+  __shared__ int sw[kHriThreads / 32];
+  const long long R = min((long long)ld_cg(&st->hcount), h.cap_rows);
+  for (long long i = blockIdx.x; i < R; i += gridDim.x) {
+    const int v = h.hrow[i];
+    if (h.hid[v] != (int)i) continue;  // uniform per CTA
+    const long long o = g.off[v];
+    const int L = g.len[v];
+    const int pv = g.prop[v];
+    const long long base = h.hoff[i];
+    const long long room = h.hoff[i + 1] - base;
+    int nh = 0;
+    for (int s = threadIdx.x; s < L; s += kHriThreads) {
+      const int u = g.adj[o + s];
+      if (u >= 0 && is_prior(g.prop[u], u, pv, v)) ++nh;
+    }
+    nh = (int)warp_sum_ll(nh);
+    if (lane_id() == 0) sw[warp_id()] = nh;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int t = 0;
+      for (int w = 0; w < kHriThreads / 32; ++w) t += sw[w];
+      s_cur[0] = 0;
+      s_cur[1] = t;
+      h.hsplit[i] = t;
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < L; s += kHriThreads) {
+      const int u = g.adj[o + s];
+      if (u < 0) continue;
+      const int pos = atomicAdd(&s_cur[is_prior(g.prop[u], u, pv, v) ? 0 : 1], 1);
+      if (pos < room)
+        h.pairs[base + pos] = (unsigned)u;
+      else
+        atomicOr(&st->status, ST_OVERFLOW);
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
-cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, cudaStream_t s) {
+cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, int variant, cudaStream_t s) {
   if (h.min_live <= 0 || g.n <= 0) return cudaSuccess;
   long long b = ((long long)g.n + kHriThreads - 1) / kHriThreads;
   if (b > 148 * 16) b = 148 * 16;
   hri_classify_kernel<<<(unsigned)b, kHriThreads, 0, s>>>(g, h, st);
   hri_offsets_kernel<<<1, kHriThreads, 0, s>>>(g, h, st);
-  hri_fill_kernel<<<148 * 4, kHriThreads, 0, s>>>(g, h, st);
+  if (variant == DC_HB)
+    hri_split_kernel<<<148 * 4, kHriThreads, 0, s>>>(g, h, st);
+  else
+    hri_fill_kernel<<<148 * 4, kHriThreads, 0, s>>>(g, h, st);
   return cudaGetLastError();
 }
 

@@ -166,6 +166,8 @@ struct HriBufs {
   unsigned* bmF;              // n/32 + 1: colour changed since the index was built
   int2* alist;                // cap_a: (vertex, chunk) of first changes, for the append phase
   int* hist;                  // cap_hist * kHriBins: row i's neighbour count per colour at build time
+  int* hsplit;                // HB, cap_rows: row i's copy holds its prior neighbours first, hsplit[i]
+                              // of them, then the rest
   long long cap_rows, cap_pairs, cap_exc, cap_a, cap_hist;
   int min_live;               // 0: no index
 };
@@ -225,7 +227,8 @@ cudaError_t launch_range_gather(const GraphDev& g, int base, int v0, int nv, con
 cudaError_t launch_range_scatter(const GraphDev& g, int base, int v0, int nv, const long long* pre, const int* in,
                                  cudaStream_t s);
 cudaError_t launch_fill(int* p, long long count, int value, cudaStream_t s);
-// Builds the heavy-row index of the current graph and colours (dc_hri.cu).
-cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, cudaStream_t s);
+// Builds the heavy-row index of the current graph and colours (dc_hri.cu):
+// HI orders rows by colour, HB splits them by LDF priority.
+cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, int variant, cudaStream_t s);
 
 }  // namespace dc

@@ -145,6 +145,7 @@ struct Env {
   HriBufs hri;
   bool hri_on;
   bool hri_mex;          // the loop's mex may use the index (its change lists are complete)
+  bool hri_split;        // HB: indexed rows list their prior neighbours first
   long long read_delta;  // entries read minus entries the rules cover
   // batched mode (all nullptr for one graph)
   const int* gid;
@@ -289,8 +290,56 @@ __device__ bool reduce_heavy(Env& E, Shared& sh, int4 un, int* out) {
   return true;
 }
 
+// HB mex over the prior neighbours of an indexed row v (seeding and loop):
+// only the first hsplit entries of its copy are prior to v, so only their
+// colours are gathered.  The whole row is handled by its first unit.
+__device__ bool reduce_split(Env& E, Shared& sh, int4 un, int* out) {
+  const HriBufs& H = E.hri;
+  const int v = un.x;
+  const int hi = H.hid[v];
+  if (hi < 0) return false;
+  if (un.y != 0) return true;
+  const long long pb = H.hoff[hi];
+  const long long live = H.hoff[hi + 1] - pb;
+  const int nh = H.hsplit[hi];
+  if (lane_id() == 0) E.my_scanned += live;  // the rule covers every live entry
+  unsigned* sm = sh.mask[warp_id()];
+  const int nw = mask_words(nh + 1, M_MEX_ALL);  // the mex of nh colours is at most nh
+  for (int k = lane_id(); k < nw; k += 32) sm[k] = 0;
+  __syncwarp();
+  unsigned long long lm = 0;
+  for (int r0 = 0; r0 < nh; r0 += 128) {
+    int cc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int idx = r0 + j * 32 + lane_id();
+      cc[j] = idx < nh ? (int)((unsigned)E.cp[(int)(unsigned)H.pairs[pb + idx]] & (unsigned)kColorMask) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = cc[j];
+      if (c < 0) continue;
+      if (c < 64)
+        lm |= 1ull << c;
+      else if (c < nw * 32)
+        atomicOr(&sm[c >> 5], 1u << (c & 31));
+    }
+  }
+  fold_low(sm, lm);
+  int r = first_zero(sm, nw);
+  __syncwarp();
+  if (r < 0) r = slow_mex(E, sm, v, M_MEX_PRIOR);  // every colour of the window present
+  if (lane_id() == 0) {
+    out[v] = r;
+    E.read_delta += nh - live;
+  }
+  __syncwarp();
+  return true;
+}
+
 __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, int mode, int* out) {
   if (E.hri_mex && mode == M_MEX_ALL && reduce_heavy(E, sh, un, out)) return;
+  if (E.hri_split && mode == M_MEX_PRIOR && reduce_split(E, sh, un, out)) return;
   const GraphDev& g = E.g;
   const int v = un.x, chunk = un.y, ms = un.z, nch = un.w;
   const int L = g.len[v];
@@ -921,6 +970,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.hri = p.hri;
   E.hri_on = V == DC_HI && p.hri.min_live > 0;
   E.hri_mex = false;  // set once the seeding's changes are in the change lists
+  E.hri_split = V == DC_HB && p.hri.min_live > 0;
   E.read_delta = 0;
   DevState* st = p.st;
   const GraphDev& g = E.g;

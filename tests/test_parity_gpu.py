@@ -310,21 +310,23 @@ def test_greedy_initial_colouring_of_the_resident_graph():
     ctx.close()
 
 
+@pytest.mark.parametrize("variant,ov", VARIANTS)
 @pytest.mark.parametrize("min_live,unit_slots", [(64, 128), (256, 2048), (-1, 2048)])
-def test_heavy_row_index_matches_oracle(min_live, unit_slots):
-    """HI with the per-batch colour index of heavy rows (many rows indexed,
-    rows split over many units, and the index off): colours, iterations,
+def test_heavy_row_index_matches_oracle(variant, ov, min_live, unit_slots):
+    """The per-batch index of heavy rows (HI: neighbours ordered by colour
+    plus change lists; HB: prior neighbours first) with many rows indexed,
+    rows split over many units, and the index off: colours, iterations,
     frontier sizes and covered entries stay those of the oracle, while the
     entries actually read drop when the index is on."""
     n, a, b = rmat_graph(14, 16, seed=5)
     col = dc.greedy_color(n, a, b)
     es = dc.EdgeSet(n, a, b)
-    ctx = gpu_ctx(dc.HI, n, a, b, col, unit_slots=unit_slots, heavy_min_live=min_live)
+    ctx = gpu_ctx(variant, n, a, b, col, unit_slots=unit_slots, heavy_min_live=min_live)
     g = oracle_graph(n, a, b, col)
     read = scanned = 0
     for i in range(4):
         ch = es.sample_batch(4000, 4000, mode=dc.INS_RMAT, scale=14, seed=40 + i)
-        rc, so = g.apply_batch(ch, po.HI, po.SNAPSHOT)
+        rc, so = g.apply_batch(ch, ov, po.SNAPSHOT)
         sg = ctx.apply_batch(to_dc_changes(ch))
         check_same(ctx, g, sg, so)
         read += sg.slots_read
