@@ -57,7 +57,7 @@ __global__ void hri_offsets_kernel(GraphDev g, HriBufs h, DevState* st) {
   for (long long c0 = 0; c0 < R; c0 += kHriThreads) {
     const long long i = c0 + threadIdx.x;
     const int L = i < R ? g.live[h.hrow[i]] : 0;
-    const long long xp = i < R ? xcap(L) : 0;
+    const long long xp = (i < R && h.xv) ? xcap(L) : 0;  // HB keeps no change lists
     // two block scans (pairs, list capacity)
     long long vals[2] = {(long long)L, xp};
     long long excl[2];
