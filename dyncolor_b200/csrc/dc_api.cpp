@@ -399,10 +399,12 @@ dc_status enqueue_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const
     const size_t b0 = offsetof(DevState, bar_arrived);
     const size_t b1 = offsetof(DevState, wctr) + sizeof(((DevState*)nullptr)->wctr);
     DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
-    if (ctx->hri.min_live > 0)
-      DC_CK(launch_hri_build(graph_dev(ctx), ctx->hri, ctx->st, ctx->opt.variant, ctx->stream));
     RecolorParams rp = recolor_params(ctx, d_ch, k);
     rp.k_dev = k_dev;
+    if (ctx->use_index)
+      DC_CK(launch_hri_build(graph_dev(ctx), ctx->hri, ctx->st, ctx->opt.variant, ctx->stream));
+    else
+      rp.hri.min_live = 0;  // this batch scans every row
     DC_CK(launch_recolor(rp, ctx->grid_recolor, ctx->stream));
   }
   if (events) DC_CK(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -420,8 +422,8 @@ void drop_graph(dc_ctx* ctx) {
 // Captures the batch sequence (lines in ctx->d_ch, count in st->batch_k)
 // into a CUDA graph; recaptured whenever a buffer it names was reallocated.
 dc_status ensure_graph(dc_ctx* ctx) {
-  const long long key[5] = {ctx->kcap, ctx->k_pool_cap, ctx->rc_pool_cap, ctx->ngraphs,
-                            (long long)(uintptr_t)ctx->d_ch};
+  const long long key[6] = {ctx->kcap, ctx->k_pool_cap, ctx->rc_pool_cap, ctx->ngraphs,
+                            (long long)(uintptr_t)ctx->d_ch, ctx->use_index ? 1 : 0};
   if (ctx->gexec && std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) return DC_OK;
   drop_graph(ctx);
   DC_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -449,6 +451,11 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   dc_status s;
   if ((s = ensure_batch_scratch(ctx, k)) != DC_OK) return s;
   if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+  // The heavy-row index is rebuilt for every row of the graph at each
+  // launch; it pays off when the batch is large enough to start long
+  // cascades through those rows, and a small batch on a big graph (or one
+  // graph's batch in a pool of many) would mostly pay for the build.
+  ctx->use_index = recolor && ctx->hri.min_live > 0 && k * kIndexBatchRatio >= (long long)ctx->n;
   bool compacted = false;
   for (int attempt = 0;; ++attempt) {
     const bool graph = ctx->opt.cuda_graph && recolor && attempt == 0;

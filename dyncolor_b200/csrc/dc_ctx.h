@@ -96,7 +96,8 @@ struct dc_ctx {
   // captured batch graph
   cudaGraph_t cgraph = nullptr;
   cudaGraphExec_t gexec = nullptr;
-  long long graph_key[5] = {0, 0, 0, 0, 0};
+  long long graph_key[6] = {0, 0, 0, 0, 0, 0};
+  bool use_index = false;  // this batch builds and uses the heavy-row index
   long long* h_k = nullptr;  // pinned line count for the captured graph
   bool last_graph = false;   // the last batch ran from the captured graph
 

@@ -154,6 +154,8 @@ struct StructParams {
 // colour color[v], and the list, instead of gathering every neighbour's
 // colour.
 constexpr int kHeavyMinLive = 2048;
+// A batch uses the index when lines * kIndexBatchRatio >= n.
+constexpr long long kIndexBatchRatio = 32;
 constexpr int kHriBins = 1024;  // exact colour order below 1023; colours >= 1023 share the first bin
 struct HriBufs {
   int* hid;                   // n: index of v's ordered copy, or -1

@@ -494,6 +494,9 @@ dc_status dc_pool_create(dc_pool** out, const dc_pool_options* opt) {
   dc_pool* P = new (std::nothrow) dc_pool();
   if (!P) return DC_E_NOMEM;
   P->opt = o;
+  // one launch serves a few of many resident graphs: an index rebuilt for
+  // the heavy rows of every resident graph would cost more than it saves
+  co.heavy_min_live = -1;
   dc_status s = dc_create(&P->u, &co);
   if (s != DC_OK) {
     delete P;

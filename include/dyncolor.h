@@ -76,9 +76,9 @@ typedef struct {
   int64_t reserve_slots; /* initial adjacency pool size hint in slots; 0: automatic */
   int32_t unit_slots;    /* adjacency slots per warp work unit (multiple of 128); 0: 2048 */
   int32_t cuda_graph;    /* 1: replay each batch's launches from a captured CUDA graph */
-  int32_t heavy_min_live; /* HI: rows with at least this many live slots get a per-batch colour
-                             index for findEligibleNeighbors; 0: 2048, < 0: off (results are the
-                             same either way) */
+  int32_t heavy_min_live; /* rows with at least this many live slots get a per-batch index (HI: by
+                             colour, HB: by priority) used by batches of at least n/32 lines;
+                             0: 2048, < 0: off.  Results are the same either way. */
   int32_t reserved[5];
 } dc_options;
 
