@@ -454,8 +454,9 @@ def run_ours(args, dist: Dist):
         "config": config(args, w),
         "e2e": {"value": total_updates / e2e_s if e2e_s > 0 else None, "unit": UNIT,
                 "h2d_bytes_per_step": 12 * k, "d2h_bytes_per_step": 4 * int(w["n"])},
-        # per batch: structural + recolour launches, and the three heavy-row index kernels
-        "gpu_launches": (5 if args.heavy_min_live >= 0 else 2) * K,
+        # per batch: structural + recolour launches, and the three heavy-row
+        # index kernels when the batch uses the index (lines * 32 >= n)
+        "gpu_launches": (5 if args.heavy_min_live >= 0 and k * 32 >= int(w["n"]) else 2) * K,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                      "traffic": traffic,
