@@ -19,9 +19,18 @@
 //     H2  mex over neighbours prior in LDF order        -> ncolor
 //     H3  commit where the colour changed; F0 += vertex
 //   loop (both), until the frontier is empty (HI) or nothing changed (HB):
-//     E   findEligibleNeighbors over F  -> next frontier Q (bitmap-deduped)
+//     E   findEligibleNeighbors over F  -> next frontier Q (deduped by a
+//         mark bit in the colour word)
 //     R   recolorNeighbor's mex over Q  -> ncolor
 //     C   commit Q (HI also saves the previous colour), Q becomes F
+//     A   (HI with the heavy-row index) vertices whose colour changed for
+//         the first time join the change lists of their indexed neighbours
+//
+// Heavy-row index (built by dc_hri.cu before the launch, for batches large
+// enough to use it): HI's E and R read an indexed row through its
+// colour-ordered copy and change list instead of gathering every
+// neighbour's colour; HB's prior-filtered mex reads only the prior part of
+// an indexed row.  Results are the same as the full scans.
 //
 // Work is split by row length: rows of <= kSmall slots ("class A") are
 // processed 32 at a time by one warp with a warp-level load-balanced search
