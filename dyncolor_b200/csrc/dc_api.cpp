@@ -221,6 +221,7 @@ StructParams struct_params(dc_ctx* ctx, const dc_change* ch, const int* la, cons
   p.cap_units = ctx->cap_units;
   p.cap_rel = ctx->cap_rel;
   p.gid = ctx->ngraphs > 0 ? ctx->gid : nullptr;
+  p.bar_timeout_ns = (unsigned long long)ctx->opt.barrier_timeout_ms * 1000000ull;
   p.st = ctx->st;
   return p;
 }
@@ -250,6 +251,7 @@ RecolorParams recolor_params(dc_ctx* ctx, const dc_change* ch, long long k) {
     p.giters = ctx->giters;
     p.gstate = ctx->gstate;
   }
+  p.bar_timeout_ns = (unsigned long long)ctx->opt.barrier_timeout_ms * 1000000ull;
   p.st = ctx->st;
   return p;
 }
@@ -507,8 +509,11 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   dc_status rc = DC_OK;
   if (h.status & ST_INVAL)
     rc = fail(ctx, DC_E_INVAL, "change line with a vertex id outside [0,n) or a self-loop");
-  else if (h.status & ST_TIMEOUT)
-    rc = fail(ctx, DC_E_TIMEOUT, "a device-side grid barrier timed out");
+  else if (h.status & ST_TIMEOUT) {
+    // the launch stopped between steps: the graph and colours are partial
+    ctx->broken = true;
+    return fail(ctx, DC_E_TIMEOUT, "a device-side grid barrier timed out");
+  }
   else if (h.status & ST_OVERFLOW)
     rc = fail(ctx, DC_E_INTERNAL, "device-side capacity guard fired");
   else if (h.status & ST_POOL)
@@ -543,6 +548,13 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
 
 bool ready(dc_ctx* ctx) { return ctx && ctx->n >= 0; }
 
+dc_status gate(dc_ctx* ctx) {
+  if (!ctx) return DC_E_INVAL;
+  if (ctx->broken) return fail(ctx, DC_E_STATE, "context unusable after a device-side wait timed out; destroy it");
+  if (ctx->n < 0) return fail(ctx, DC_E_STATE, "no graph loaded");
+  return DC_OK;
+}
+
 }  // namespace host
 }  // namespace dc
 
@@ -576,6 +588,7 @@ dc_status dc_options_default(dc_options* opt) {
   opt->reserve_slots = 0;
   opt->unit_slots = kUnitSlotsDefault;
   opt->heavy_min_live = kHeavyMinLive;
+  opt->barrier_timeout_ms = kBarrierTimeoutMsDefault;
   return DC_OK;
 }
 
@@ -595,6 +608,7 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   if (o.heavy_min_live == 0) o.heavy_min_live = kHeavyMinLive;
   if (o.heavy_min_live < 0) o.heavy_min_live = 0;  // off
   if (o.heavy_min_live > 0 && o.heavy_min_live < 64) o.heavy_min_live = 64;
+  if (o.barrier_timeout_ms <= 0) o.barrier_timeout_ms = kBarrierTimeoutMsDefault;
   dc_ctx* ctx = new (std::nothrow) dc_ctx();
   if (!ctx) return DC_E_NOMEM;
   ctx->opt = o;
@@ -700,6 +714,7 @@ void dc_destroy(dc_ctx* ctx) {
 
 dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const int32_t* b, int64_t m) {
   if (!ctx) return DC_E_INVAL;
+  if (ctx->broken) return gate(ctx);
   if (ctx->n >= 0) return fail(ctx, DC_E_STATE, "graph already loaded");
   if (n < 0 || m < 0 || (m > 0 && (!a || !b))) return fail(ctx, DC_E_INVAL, "bad graph arguments");
   // pieces of kLoadPiece lines keep the sort keys and scratch in range; the
@@ -765,7 +780,7 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
 }
 
 dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (n != ctx->n || (n > 0 && !colors)) return fail(ctx, DC_E_INVAL, "colour array size differs from n");
   for (int32_t v = 0; v < n; ++v)
     if (colors[v] < 0 || colors[v] > kColorMask)
@@ -779,7 +794,7 @@ dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
 }
 
 dc_status dc_colors_init_greedy(dc_ctx* ctx) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
   const int n = ctx->n;
@@ -851,7 +866,7 @@ dc_status dc_colors_init_greedy(dc_ctx* ctx) {
 }
 
 dc_status dc_apply_batch(dc_ctx* ctx, const dc_change* changes, int64_t k, dc_stats* out) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (k < 0 || (k > 0 && !changes)) return fail(ctx, DC_E_INVAL, "bad batch arguments");
   if (k > (1ll << 30)) return fail(ctx, DC_E_INVAL, "more than 2^30 change lines");
   if (out) std::memset(out, 0, sizeof(*out));
@@ -866,7 +881,7 @@ dc_status dc_apply_batch(dc_ctx* ctx, const dc_change* changes, int64_t k, dc_st
 }
 
 dc_status dc_apply_batch_device(dc_ctx* ctx, const dc_change* d_changes, int64_t k, dc_stats* out) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (k < 0 || (k > 0 && !d_changes)) return fail(ctx, DC_E_INVAL, "bad batch arguments");
   if (k > (1ll << 30)) return fail(ctx, DC_E_INVAL, "more than 2^30 change lines");
   if (out) std::memset(out, 0, sizeof(*out));
@@ -877,7 +892,7 @@ dc_status dc_apply_batch_device(dc_ctx* ctx, const dc_change* d_changes, int64_t
 }
 
 dc_status dc_colors_read(dc_ctx* ctx, int32_t* out, int32_t n) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (n != ctx->n || (n > 0 && !out)) return fail(ctx, DC_E_INVAL, "output size differs from n");
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
@@ -887,14 +902,14 @@ dc_status dc_colors_read(dc_ctx* ctx, int32_t* out, int32_t n) {
 }
 
 dc_status dc_colors_device(dc_ctx* ctx, int32_t** d_colors) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (!d_colors) return DC_E_INVAL;
   *d_colors = ctx->color;
   return DC_OK;
 }
 
 dc_status dc_prop_read(dc_ctx* ctx, int32_t* out, int32_t n) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (n != ctx->n || (n > 0 && !out)) return fail(ctx, DC_E_INVAL, "output size differs from n");
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
@@ -904,7 +919,7 @@ dc_status dc_prop_read(dc_ctx* ctx, int32_t* out, int32_t n) {
 }
 
 dc_status dc_validate(dc_ctx* ctx, int64_t* conflicts) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (!conflicts) return DC_E_INVAL;
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
@@ -916,7 +931,7 @@ dc_status dc_validate(dc_ctx* ctx, int64_t* conflicts) {
 }
 
 dc_status dc_neighbors(dc_ctx* ctx, int32_t v, int32_t* out, int32_t cap, int32_t* deg) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (v < 0 || v >= ctx->n || !deg || (cap > 0 && !out)) return fail(ctx, DC_E_INVAL, "bad vertex");
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
@@ -941,7 +956,7 @@ dc_status dc_neighbors(dc_ctx* ctx, int32_t v, int32_t* out, int32_t cap, int32_
 }
 
 dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (!info) return DC_E_INVAL;
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
@@ -958,7 +973,7 @@ dc_status dc_graph_info_get(dc_ctx* ctx, dc_graph_info* info) {
 }
 
 dc_status dc_compact(dc_ctx* ctx) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
   dc_status s = repack(ctx, ctx->pool_cap);
@@ -969,7 +984,7 @@ dc_status dc_compact(dc_ctx* ctx) {
 }
 
 dc_status dc_partition_set(dc_ctx* ctx, int32_t ngraphs, const int32_t* first) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (ngraphs <= 0 || !first) return fail(ctx, DC_E_INVAL, "bad partition arguments");
   if (first[0] != 0 || first[ngraphs] != ctx->n)
     return fail(ctx, DC_E_INVAL, "partition must start at 0 and end at n");
@@ -999,7 +1014,7 @@ dc_status dc_partition_set(dc_ctx* ctx, int32_t ngraphs, const int32_t* first) {
 }
 
 dc_status dc_graph_iterations(dc_ctx* ctx, int64_t* out, int32_t ngraphs) {
-  if (!ready(ctx)) return fail(ctx, DC_E_STATE, "no graph loaded");
+  if (dc_status g_ = gate(ctx)) return g_;
   if (ctx->ngraphs == 0) return fail(ctx, DC_E_STATE, "no partition set");
   if (ngraphs != ctx->ngraphs || !out) return fail(ctx, DC_E_INVAL, "output size differs from the partition");
   cudaSetDevice(ctx->device);

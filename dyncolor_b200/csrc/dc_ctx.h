@@ -22,6 +22,7 @@ struct dc_ctx {
   int grid_struct = 0;
   int grid_recolor = 0;
   std::string err;
+  bool broken = false;  // a device-side wait timed out: every later call is refused
   long long bytes = 0;  // device bytes held (dalloc / dfree)
   std::unordered_map<void*, long long> sizes;
 
@@ -177,6 +178,8 @@ dc_status packed_total(dc_ctx* ctx, long long* total, long long** scratch_out);
 dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int* lb, long long k, bool recolor,
                     dc_stats* out);
 bool ready(dc_ctx* ctx);
+// DC_OK when the context holds a graph and is usable, else the status to return.
+dc_status gate(dc_ctx* ctx);
 
 }  // namespace host
 }  // namespace dc

@@ -39,10 +39,10 @@ __device__ __forceinline__ T ld_cg(const T* p) {
 
 // Software grid barrier for a cooperative (all-CTAs-resident) launch.
 // `target` is per-CTA state starting at 0.  Every wait is bounded by
-// kBarrierTimeoutNs of globaltimer; on expiry the CTA raises ST_TIMEOUT and
-// the abort flag, and every CTA then returns false from its next wait so the
+// `timeout_ns` of globaltimer; on expiry the CTA raises ST_TIMEOUT and the
+// abort flag, and every CTA then returns false from its next wait so the
 // kernel exits instead of hanging.
-__device__ __forceinline__ bool grid_sync(DevState* st, unsigned& target) {
+__device__ __forceinline__ bool grid_sync(DevState* st, unsigned& target, unsigned long long timeout_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -59,7 +59,7 @@ __device__ __forceinline__ bool grid_sync(DevState* st, unsigned& target) {
         ok = 0;
         break;
       }
-      if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > kBarrierTimeoutNs) {
+      if ((++spins & 255u) == 0 && globaltimer_ns() - t0 > timeout_ns) {
         atomicOr(&st->status, ST_TIMEOUT);
         atomicExch(&st->bar_abort, 1u);
         ok = 0;

@@ -31,7 +31,7 @@ constexpr int kColorMask = (1 << 30) - 1;
 constexpr int kNumQueues = 6;       // logical queue counter slots
 constexpr int kUnitSlotsDefault = 2048;  // adjacency slots per warp work unit
 constexpr long long kLoadPiece = 1ll << 27;  // edge pairs per structural launch of a graph load
-constexpr unsigned long long kBarrierTimeoutNs = 20ull * 1000ull * 1000ull * 1000ull;
+constexpr int kBarrierTimeoutMsDefault = 20000;  // grid-barrier wait limit unless the options set one
 
 // Logical queue counter slots.
 enum { Q_LOOP0 = 0, Q_LOOP1 = 1, Q_LOOP2 = 2, Q_S1 = 3, Q_S2E = 4, Q_S2T = 5 };
@@ -142,6 +142,7 @@ struct StructParams {
   long long cap_units;
   long long cap_rel;
   const int* gid;        // batched mode: vertex -> graph; lines must stay inside a graph
+  unsigned long long bar_timeout_ns;  // limit of every grid-barrier wait
   DevState* st;
 };
 
@@ -198,6 +199,7 @@ struct RecolorParams {
   int* gf0;              // ngraphs: vertices each graph put in frontier F0
   int* giters;           // ngraphs: loop iterations of each graph
   int* gstate;           // ngraphs: 0 not started, 1 running, 2 done
+  unsigned long long bar_timeout_ns;  // limit of every grid-barrier wait
   DevState* st;
 };
 

@@ -10,7 +10,6 @@
 // the file-scope device array below, which every GPU that loads the library
 // holds until the process exits.
 #include <algorithm>
-#include <mutex>
 
 #include "../../include/dyncolor.h"
 #include "dc_device.cuh"
@@ -84,9 +83,6 @@ __global__ void noalloc_validate_kernel(int n, const long long* off, const int* 
   }
 }
 
-std::mutex g_setup_mu;
-unsigned int* g_scratch_ptr[64] = {nullptr};
-
 }  // namespace
 
 }  // namespace dc
@@ -98,40 +94,52 @@ extern "C" dc_status dc_validate_csr_noalloc(int32_t n, const int64_t* d_row_off
   using namespace dc;
   if (n < 0 || n > kNoAllocMaxVertices) return DC_E_INVAL;  // bitmap holds 2^24 vertices
   if (!conflicts || (n > 0 && (!d_row_off || !d_row_len || !d_adj || !d_colors))) return DC_E_INVAL;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DC_E_CUDA;
-  unsigned int* scratch = nullptr;
-  {
-    // First call on a device: look up the device address of the scratch
-    // array with that device current.  The array's name in host code is only
-    // a host-side stand-in and must never be handed to a kernel.
-    std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_ptr[dev]) {
-      void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
-        cudaGetLastError();
-        return DC_E_CUDA;
-      }
-      g_scratch_ptr[dev] = static_cast<unsigned int*>(p);
-    }
-    scratch = g_scratch_ptr[dev];
-  }
+  cudaGetLastError();  // an error left by the caller's own earlier work is not this call's
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The call waits for its stream at the end, which a capturing stream does
+  // not allow.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    return DC_E_CUDA;
+  }
+  if (cap != cudaStreamCaptureStatusNone) return DC_E_STATE;
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                 cudaSuccess) {
+    cudaGetLastError();
+    return DC_E_CUDA;
+  }
+  // The device address of the scratch array, looked up on every call with
+  // the caller's device current.  In host code the array's name is only a
+  // host-side stand-in and must never be handed to a kernel; and an address
+  // kept from an earlier call could belong to a module that a device reset
+  // has since unloaded, so none is kept.  The lookup allocates nothing.
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+    cudaGetLastError();
+    return DC_E_CUDA;
+  }
+  unsigned int* scratch = static_cast<unsigned int*>(p);
   // The array keeps the previous call's contents: clear the header and the
   // bitmap words this call uses.
   const long long words = kHeaderWords + ((long long)n + 31) / 32;
   const int cgrid = (int)std::min<long long>((words + kNoAllocThreads - 1) / kNoAllocThreads, 1024);
   noalloc_clear_kernel<<<cgrid, kNoAllocThreads, 0, s>>>(scratch, words);
   if (n > 0) {
-    const int vgrid = (int)std::min<long long>(((long long)n * 32 + kNoAllocThreads - 1) / kNoAllocThreads, 148 * 16);
+    const long long per_sm = 2048 / kNoAllocThreads;  // resident blocks of 256 threads per SM
+    const int vgrid = (int)std::min<long long>(((long long)n * 32 + kNoAllocThreads - 1) / kNoAllocThreads,
+                                               (long long)std::max(sms, 1) * per_sm);
     noalloc_validate_kernel<<<vgrid, kNoAllocThreads, 0, s>>>(
         n, reinterpret_cast<const long long*>(d_row_off), d_row_len, d_adj, d_colors, scratch);
   }
   if (cudaGetLastError() != cudaSuccess) return DC_E_CUDA;
   unsigned int head[6];
   if (cudaMemcpyAsync(head, scratch, sizeof(head), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
+      cudaStreamSynchronize(s) != cudaSuccess) {
+    cudaGetLastError();
     return DC_E_CUDA;
+  }
   if (head[5] != 0u) return DC_E_INVAL;  // negative colour or neighbour id outside [0, n)
   *conflicts = (int64_t)(((unsigned long long)head[1] << 32) | head[0]);
   if (conflicted_vertices) *conflicted_vertices = (int64_t)(((unsigned long long)head[3] << 32) | head[2]);

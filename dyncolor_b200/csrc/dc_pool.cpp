@@ -450,7 +450,10 @@ dc_status restore(dc_pool* P, int gi, const std::vector<char>& locked) {
   return DC_OK;
 }
 
-bool pool_ready(const dc_pool* P) { return P && P->u; }
+bool pool_ready(const dc_pool* P) { return P && P->u && !P->u->broken; }
+// Status for a pool that is not ready: DC_E_STATE after a device-side wait
+// timed out in its union context, else DC_E_INVAL.
+dc_status pool_gate(const dc_pool* P) { return (P && P->u && P->u->broken) ? DC_E_STATE : DC_E_INVAL; }
 
 }  // namespace
 
@@ -562,7 +565,8 @@ void dc_pool_destroy(dc_pool* P) {
 
 dc_status dc_pool_add_graph(dc_pool* P, int32_t n, const int32_t* a, const int32_t* b, int64_t m,
                             const int32_t* colors, int32_t* graph) {
-  if (!pool_ready(P) || !graph) return DC_E_INVAL;
+  if (!pool_ready(P)) return pool_gate(P);
+  if (!graph) return DC_E_INVAL;
   dc_ctx* ctx = P->u;
   if (n < 0 || m < 0 || (m > 0 && (!a || !b)) || (n > 0 && !colors))
     return pfail(P, DC_E_INVAL, "bad graph arguments");
@@ -659,7 +663,7 @@ dc_status dc_pool_add_graph(dc_pool* P, int32_t n, const int32_t* a, const int32
 
 dc_status dc_pool_apply(dc_pool* P, const dc_pool_request* reqs, int32_t count, dc_pool_result* results,
                         dc_stats* stats) {
-  if (!pool_ready(P)) return DC_E_INVAL;
+  if (!pool_ready(P)) return pool_gate(P);
   dc_ctx* ctx = P->u;
   if (stats) std::memset(stats, 0, sizeof(*stats));
   if (count < 0 || (count > 0 && !reqs)) return pfail(P, DC_E_INVAL, "bad request arguments");
@@ -739,7 +743,7 @@ dc_status dc_pool_apply(dc_pool* P, const dc_pool_request* reqs, int32_t count, 
 }
 
 dc_status dc_pool_colors_read(dc_pool* P, int32_t graph, int32_t* out, int32_t n) {
-  if (!pool_ready(P)) return DC_E_INVAL;
+  if (!pool_ready(P)) return pool_gate(P);
   dc_ctx* ctx = P->u;
   if (graph < 0 || graph >= (int)P->graphs.size()) return pfail(P, DC_E_INVAL, "unknown graph");
   const PGraph& g = P->graphs[(size_t)graph];
@@ -757,7 +761,7 @@ dc_status dc_pool_colors_read(dc_pool* P, int32_t graph, int32_t* out, int32_t n
 }
 
 dc_status dc_pool_spill(dc_pool* P, int32_t graph) {
-  if (!pool_ready(P)) return DC_E_INVAL;
+  if (!pool_ready(P)) return pool_gate(P);
   if (graph < 0 || graph >= (int)P->graphs.size()) return pfail(P, DC_E_INVAL, "unknown graph");
   cudaSetDevice(P->u->device);
   cudaGetLastError();
@@ -765,7 +769,7 @@ dc_status dc_pool_spill(dc_pool* P, int32_t graph) {
 }
 
 dc_status dc_pool_graph_size(dc_pool* P, int32_t graph, int32_t* n, int64_t* slots, int32_t* resident) {
-  if (!pool_ready(P)) return DC_E_INVAL;
+  if (!pool_ready(P)) return pool_gate(P);
   if (graph < 0 || graph >= (int)P->graphs.size()) return pfail(P, DC_E_INVAL, "unknown graph");
   const PGraph& g = P->graphs[(size_t)graph];
   if (n) *n = g.n;
@@ -775,7 +779,8 @@ dc_status dc_pool_graph_size(dc_pool* P, int32_t graph, int32_t* n, int64_t* slo
 }
 
 dc_status dc_pool_info_get(dc_pool* P, dc_pool_info* info) {
-  if (!pool_ready(P) || !info) return DC_E_INVAL;
+  if (!pool_ready(P)) return pool_gate(P);
+  if (!info) return DC_E_INVAL;
   cudaSetDevice(P->u->device);
   cudaGetLastError();
   long long used = 0;

@@ -1030,15 +1030,15 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       const bool claim = t >= 0 && mark_bit(p.bmA, t);
       warp_push(B2, &st->q[Q_S1], g.len, claim ? t : -1, true, M_MEX_ALL, E.CH, &st->status);
     }
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // D2
     phase_reduce(E, sh, B2, &st->q[Q_S1], ctr(), M_MEX_ALL, p.ncolor);
     ++ps;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // D3
     phase_commit(E, B2, &st->q[Q_S1], C_SEED_DEL, &B0, &st->q[Q_LOOP0], gwarp, nwarps,
                  &st->seed_targets, nullptr);
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // I1: insertions still monochromatic -> both endpoints
     for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
@@ -1056,11 +1056,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       const bool cb = b >= 0 && mark_bit(p.bmA, b);
       warp_push(B2, &st->q[Q_S2E], g.len, cb ? b : -1, false, M_DISTINCT, E.CH, &st->status);
     }
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // I2: saturation sizes
     phase_reduce(E, sh, B2, &st->q[Q_S2E], ctr(), M_DISTINCT, p.sat);
     ++ps;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // I3: targets; release the endpoint set
     for (long long i0 = gwarp * 32; i0 < K; i0 += nwarps * 32) {
       const long long i = i0 + lane_id();
@@ -1074,15 +1074,15 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     }
     phase_commit(E, B2, &st->q[Q_S2E], C_CLEAR_A, nullptr, nullptr, gwarp, nwarps, nullptr,
                  nullptr);
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // I4
     phase_reduce(E, sh, B1, &st->q[Q_S2T], ctr(), M_MEX_ALL, p.ncolor);
     ++ps;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // I5
     phase_commit(E, B1, &st->q[Q_S2T], C_SEED_INS, &B0, &st->q[Q_LOOP0], gwarp, nwarps,
                  &st->seed_targets, nullptr);
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   } else {
     // packed (degree property, colour) words for this launch's gathers;
     // the barrier after H1 publishes them before H2 reads any
@@ -1104,15 +1104,15 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       const bool cb = b >= 0 && mark_bit(p.bmA, b);
       warp_push(B2, &st->q[Q_S1], g.len, cb ? b : -1, true, M_MEX_ALL, E.CH, &st->status);
     }
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // H2
     phase_reduce(E, sh, B2, &st->q[Q_S1], ctr(), M_MEX_PRIOR, p.ncolor);
     ++ps;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // H3
     phase_commit(E, B2, &st->q[Q_S1], C_SEED_HB, &B0, &st->q[Q_LOOP0], gwarp, nwarps,
                  &st->seed_targets, nullptr);
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   }
   // F0 is complete: release its marks so the loop can mark into bmB.
   phase_commit(E, B0, &st->q[Q_LOOP0], C_CLEAR_B, nullptr, nullptr, gwarp, nwarps, nullptr,
@@ -1121,13 +1121,13 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     // a graph whose seeding recoloured nothing never enters the loop
     for (long long gg = gtid; gg < p.ngraphs; gg += gthreads) p.gstate[gg] = ld_cg(&p.gf0[gg]) > 0 ? 1 : 2;
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   // rows of vertices the seeding recoloured join their indexed neighbours'
   // change lists before the loop reads them
   if (E.hri_on && ld_cg(&st->a_count) > 0) {
     phase_append(E, ctr());
     ++ps;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   }
   E.hri_mex = E.hri_on;
   lap(0);
@@ -1179,7 +1179,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       }
       phase_expand(E, sh, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
       ++ps;
-      if (!grid_sync(st, bar)) return;
+      if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       lap(1);
       const QCount* nc = &st->q[ns];
       const long long nq = (long long)(ld_cg(&nc->countA) + ld_cg(&nc->countU));
@@ -1201,16 +1201,16 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       }
       phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
       ++ps;
-      if (!grid_sync(st, bar)) return;
+      if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       lap(2);
       // C
       phase_commit(E, p.qb[nb], nc, C_LOOP, nullptr, nullptr, gwarp, nwarps, &st->frontier_total,
                    &st->chg[it & 1]);
-      if (!grid_sync(st, bar)) return;
+      if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       if (E.hri_on && ld_cg(&st->a_count) > 0) {
         phase_append(E, ctr());
         ++ps;
-        if (!grid_sync(st, bar)) return;
+        if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       }
       lap(3);
       if (V == DC_HB && ld_cg(&st->chg[it & 1]) == 0) break;

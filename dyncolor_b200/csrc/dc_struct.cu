@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
     const long long s = warp_sum_ll(nv);
     if (lane == 0 && s) atomicAdd(&st->nvalid, (unsigned long long)s);
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   if (ld_cg(&st->status) & ST_INVAL) return;  // nothing modified
   const long long NV = 2 * (long long)ld_cg(&st->nvalid);
 
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       atomicAdd(&s_hist[(unsigned)(src[i] >> shift) & 255u], 1u);
     __syncthreads();
     for (int d = tid; d < 256; d += kThreads) p.hist[(long long)blockIdx.x * 256 + d] = s_hist[d];
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // P2: for each digit, exclusive prefix over CTAs
     for (int d = blockIdx.x; d < 256; d += G) {
       unsigned run = 0;
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       }
       if (tid == 0) p.dscan[(long long)G * 256 + d] = run;
     }
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     // P3: stable scatter
     {
       const int v = tid < 256 ? (int)ld_cg(&p.dscan[(long long)G * 256 + tid]) : 0;
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
           __syncthreads();
         }
       }
-      if (!grid_sync(st, bar)) return;
+      if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       if (!skip) {
         unsigned long long* t = src;
         src = dst;
@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
     int tot;
     block_excl_scan(cnt, s_sw, &tot);
     if (tid == 0) p.cta_cnt[blockIdx.x] = (unsigned)tot;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     long long base, total;
     cta_prefix(p.cta_cnt, &base, &total, s_swll);
     if (blockIdx.x == 0 && tid == 0) st->nnet = (unsigned long long)total;
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       run += tt;
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   const long long NN = (long long)ld_cg(&st->nnet);
 
   // ---------------- S2: touched rows ----------------
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
     int tot;
     block_excl_scan(cnt, s_sw, &tot);
     if (tid == 0) p.cta_cnt[blockIdx.x] = (unsigned)tot;
-    if (!grid_sync(st, bar)) return;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
     long long base, total;
     cta_prefix(p.cta_cnt, &base, &total, s_swll);
     if (blockIdx.x == 0 && tid == 0) {
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       run += tt;
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   const long long NT_ = (long long)ld_cg(&st->ntouched);
 
   // ---------------- S3a: row-scan units ----------------
@@ -306,7 +306,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
         atomicOr(&st->status, ST_OVERFLOW);
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   if (ld_cg(&st->status) & ST_OVERFLOW) return;
 
   // ---------------- S3b: scan touched rows ----------------
@@ -356,14 +356,14 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       if (lane == 0 && nd) atomicAdd(&p.rowdel[t], (int)nd);
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
 
   // ---------------- S4a: ranks of new neighbours ----------------
   for (long long j = gtid; j < NN; j += gthreads) {
     const unsigned long long kj = p.net[j];
     if (key_op(kj) == 1 && !p.present[j]) p.rank[j] = atomicAdd(&p.tins[p.tof[j]], 1);
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
 
   // ---------------- S4b: per-row capacity decisions ----------------
   {
@@ -422,7 +422,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       if (rel) atomicAdd(&st->rows_relocated, (unsigned long long)rel);
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
   {
     // Uniform decision: every CTA reads the pool counter before anyone
     // could restore it (the restore happens after one more barrier).
@@ -430,7 +430,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
                       (ld_cg(&st->status) & ST_OVERFLOW) != 0;
     if (fail) {
       if (blockIdx.x == 0 && tid == 0) atomicOr(&st->status, ST_POOL);
-      if (!grid_sync(st, bar)) return;
+      if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       if (blockIdx.x == 0 && tid == 0) st->pool_used = st->pool_used_start;
       return;
     }
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       }
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
 
   // ---------------- S6: relocation copies + appends ----------------
   {
@@ -494,7 +494,7 @@ __global__ void __launch_bounds__(kThreads) struct_kernel(StructParams p) {
       }
     }
   }
-  if (!grid_sync(st, bar)) return;
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
 
   // ---------------- S7: commit row metadata ----------------
   for (long long t = gtid; t < NT_; t += gthreads) {

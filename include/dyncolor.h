@@ -48,7 +48,8 @@ typedef enum {
   DC_E_CUDA = 3,       /* a CUDA runtime call failed (see dc_last_error) */
   DC_E_ITER_LIMIT = 4, /* the recolour loop hit options.iter_cap; colours are partial */
   DC_E_STATE = 5,      /* call out of order (e.g. apply before load) */
-  DC_E_TIMEOUT = 6,    /* a device-side wait gave up (grid barrier); context unusable */
+  DC_E_TIMEOUT = 6,    /* a device-side wait gave up (grid barrier); the context refuses every
+                          later call but dc_destroy/dc_last_error with DC_E_STATE */
   DC_E_INTERNAL = 7    /* a device-side capacity guard fired */
 } dc_status;
 
@@ -79,7 +80,10 @@ typedef struct {
   int32_t heavy_min_live; /* rows with at least this many live slots get a per-batch index (HI: by
                              colour, HB: by priority) used by batches of at least n/32 lines;
                              0: 2048, < 0: off.  Results are the same either way. */
-  int32_t reserved[5];
+  int32_t barrier_timeout_ms; /* limit of every device-side grid-barrier wait; 0: 20,000 ms.  A wait
+                                 that runs out ends the launch with DC_E_TIMEOUT instead of hanging,
+                                 and the context then refuses further work (DC_E_STATE). */
+  int32_t reserved[4];
 } dc_options;
 
 typedef struct {
@@ -190,14 +194,17 @@ dc_status dc_compact(dc_ctx* ctx);
  * d_row_len[r] entries from d_adj[d_row_off[r]]; negative entries are
  * skipped as deleted) on the current device and `stream`, and returns the
  * number of monochromatic edges {u,v}, of vertices on such an edge, and the
- * largest colour.  n must not exceed 16,777,216 (2^24): the scratch bitmap
- * is a fixed 2 MiB device array inside the library, held by every GPU that
- * loads it until the process exits.  The first call on a device looks that
- * array up (cudaGetSymbolAddress), so make it before any stream capture.
- * All calls share the array: calls that overlap on the GPU (other streams,
- * other host threads) race.  Synchronises `stream` before returning.
- * DC_E_INVAL: n out of range, a negative colour or a neighbour id outside
- * [0, n). */
+ * largest colour.  A row that lists the same neighbour twice counts a
+ * monochromatic edge once per copy (the library's own rows never do).
+ * n must not exceed 16,777,216 (2^24): the scratch bitmap is a fixed 2 MiB
+ * device array inside the library, held by every GPU that loads it until
+ * the process exits.  Every call looks up that array's device address with
+ * the caller's device current (no allocation).  All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * The call waits for `stream` before returning, so it must not be made on a
+ * stream that is being captured (DC_E_STATE).  conflicted_vertices and
+ * max_color may be NULL.  DC_E_INVAL: n out of range, a negative colour or a
+ * neighbour id outside [0, n). */
 dc_status dc_validate_csr_noalloc(int32_t n, const int64_t* d_row_off, const int32_t* d_row_len,
                                   const int32_t* d_adj, const int32_t* d_colors, void* stream,
                                   int64_t* conflicts, int64_t* conflicted_vertices,

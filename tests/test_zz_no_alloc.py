@@ -74,3 +74,47 @@ def test_noalloc_validate_rejects_bad_sizes():
     conf = C.c_int64()
     assert f((1 << 24) + 1, None, None, None, None, None, C.byref(conf), None, None) == dc.E_INVAL
     assert f(-1, None, None, None, None, None, C.byref(conf), None, None) == dc.E_INVAL
+
+
+def test_noalloc_validate_skips_deleted_entries_and_flags_bad_input():
+    """Deleted (-1) entries are skipped; a negative colour or a neighbour id
+    outside [0, n) gives E_INVAL; the optional outputs may be NULL.  Every
+    case stays inside the caller's arrays (the kernel checks an id before it
+    reads that neighbour's colour)."""
+    import torch
+
+    f = _bind()
+    n, a, b = rmat_graph(11, 8, seed=22)
+    off, deg, adj = _csr(n, a, b)
+    rng = np.random.default_rng(9)
+    colors = rng.integers(0, 6, n).astype(np.int32)
+    # delete about a third of the entries in place (both directions of an edge
+    # need not go together: each live directed entry u > v counts once)
+    adj_del = adj.copy()
+    adj_del[rng.random(len(adj)) < 0.33] = -1
+    src = np.repeat(np.arange(n), deg)
+    live = adj_del >= 0
+    u, v = adj_del[live], src[live]
+    want = int(np.count_nonzero((u > v) & (colors[u] == colors[v])))
+    rc, conf, verts, cmax = _noalloc(f, torch, n, off, deg, adj_del, colors)
+    assert rc == dc.OK and conf == want and cmax == int(colors.max())
+    mono = (u > v) & (colors[u] == colors[v])
+    assert verts == len(np.unique(np.concatenate([u[mono], v[mono]])))
+    # NULL optional outputs
+    d = [torch.from_numpy(x).cuda() for x in (off, deg, adj_del, colors)]
+    torch.cuda.synchronize()
+    conf2 = C.c_int64(-1)
+    assert f(n, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(), None,
+             C.byref(conf2), None, None) == dc.OK
+    assert conf2.value == want
+    # a negative colour
+    bad_col = colors.copy()
+    bad_col[7] = -1
+    assert _noalloc(f, torch, n, off, deg, adj, bad_col)[0] == dc.E_INVAL
+    # a neighbour id equal to n
+    bad_adj = adj.copy()
+    bad_adj[3] = n
+    assert _noalloc(f, torch, n, off, deg, bad_adj, colors)[0] == dc.E_INVAL
+    # and the next clean call is unaffected by the flags the bad ones left
+    rc, conf, _, _ = _noalloc(f, torch, n, off, deg, adj_del, colors)
+    assert rc == dc.OK and conf == want
