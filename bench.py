@@ -52,14 +52,20 @@ def parse_args():
     ap.add_argument("--edgefactor", type=int, default=16)
     ap.add_argument("--batch", type=int, default=1_000_000)
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--cpu-sample", type=int, default=20_000,
-                    help="change lines of the bounded CPU-baseline sample")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--ref-iter-cap", type=int, default=400)
-    ap.add_argument("--ref-sample", type=int, default=5_000,
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the oracle replay of the first batch (the parity check and the CPU baseline)")
+    ap.add_argument("--no-further-configs", action="store_true",
+                    help="skip the other single-graph configurations reported under detail.configs")
+    ap.add_argument("--cl-vertices", type=int, default=4_000_000, help="skewed-degree configuration: vertices")
+    ap.add_argument("--cl-max-deg", type=float, default=360_000.0,
+                    help="skewed-degree configuration: Chung-Lu weight of the largest vertex")
+    ap.add_argument("--ref-iter-cap", type=int, default=2000)
+    ap.add_argument("--ref-sample", type=int, default=1_000,
                     help="reference arm: change lines of each step's bounded sample")
-    ap.add_argument("--ref-step-budget-ms", type=float, default=5_000.0,
+    ap.add_argument("--ref-step-budget-ms", type=float, default=20_000.0,
                     help="reference arm: a step's loop stops once its timed work passes this budget")
+    ap.add_argument("--ref-max-fail", type=int, default=3,
+                    help="reference arm: stop after this many unconverged steps in a row")
     ap.add_argument("--unit-slots", type=int, default=0, help="adjacency slots per warp work unit (0: library default)")
     ap.add_argument("--blocks-per-sm", type=int, default=0, help="persistent CTAs per SM (0: from occupancy)")
     ap.add_argument("--heavy-min-live", type=int, default=0,
@@ -155,17 +161,46 @@ def workload_dir(args, dist: Dist) -> str:
                         f"dcbench_{args.scale}_{args.edgefactor}_{args.batch}_{args.seed}_{port}_{os.getppid() if dist.world > 1 else os.getpid()}")
 
 
-def build_workload(args, nbatches: int):
-    import dyncolor_b200 as dc
+class _ProductGen:
+    """Workload generators of the product library (libdyncolor.so)."""
 
+    def __init__(self):
+        import dyncolor_b200 as dc
+
+        self.rmat = lambda scale, m, seed: dc.rmat(scale, m, seed=seed)
+        self.chung_lu = lambda n, g, avg, mx, seed: dc.chung_lu(n, g, avg, mx, seed=seed)
+        self.dedup = dc.dedup
+        self.greedy_color = dc.greedy_color
+        self.EdgeSet = dc.EdgeSet
+        self.INS_RMAT, self.INS_DEGREE = dc.INS_RMAT, dc.INS_DEGREE
+
+
+class _CheckerGen:
+    """The same generators compiled into the checker library (liboracle.so),
+    for the reference arm, which must not load libdyncolor.so."""
+
+    def __init__(self):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+
+        self.rmat = lambda scale, m, seed: po.gen_rmat(scale, m, seed=seed)
+        self.chung_lu = lambda n, g, avg, mx, seed: po.gen_chung_lu(n, g, avg, mx, seed=seed)
+        self.dedup = po.gen_dedup
+        self.greedy_color = po.gen_greedy_color
+        self.EdgeSet = po.GenEdgeSet
+        self.INS_RMAT, self.INS_DEGREE = po.INS_RMAT, po.INS_DEGREE
+
+
+def build_workload(args, nbatches: int, gen=None):
+    gen = gen or _ProductGen()
     n = 1 << args.scale
     t0 = time.time()
-    a, b = dc.rmat(args.scale, args.edgefactor * n, seed=args.seed)
-    a, b = dc.dedup(n, a, b)
-    colors = dc.greedy_color(n, a, b)
-    es = dc.EdgeSet(n, a, b)
+    a, b = gen.rmat(args.scale, args.edgefactor * n, args.seed)
+    a, b = gen.dedup(n, a, b)
+    colors = gen.greedy_color(n, a, b)
+    es = gen.EdgeSet(n, a, b)
     half = args.batch // 2
-    batches = [es.sample_batch(half, args.batch - half, mode=dc.INS_RMAT, scale=args.scale,
+    batches = [es.sample_batch(half, args.batch - half, mode=gen.INS_RMAT, scale=args.scale,
                                seed=args.seed * 1000 + i) for i in range(nbatches)]
     return {"n": n, "a": a, "b": b, "colors": colors, "batches": batches,
             "gen_s": time.time() - t0}
@@ -271,54 +306,124 @@ def hbm_peak():
 
 
 # DRAM bytes (read + write) per covered adjacency entry of the recolour
-# launch, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum,
-# one pass) of this bench's own default workload: R-MAT scale 24, 1 M-line
-# batches, HI, heavy-row index on: 302.6 GB for 168.5 G covered entries
-# (32.1 G of them actually read).
+# launch, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum)
+# of this bench's workloads; keyed by (variant, scale, edge factor, lines).
+# The summary that each figure comes from is in profiles/.
 MEASURED_DRAM_BYTES_PER_ENTRY = {("hi", 24, 16, 1_000_000): 1.80}
 
 
-def load_traffic(args):
-    """Measured DRAM bytes per scanned entry for this workload, or None."""
-    return MEASURED_DRAM_BYTES_PER_ENTRY.get((args.variant, args.scale, args.edgefactor, args.batch))
+def load_traffic(variant: str, scale: int, ef: int, lines: int):
+    """Measured DRAM bytes per covered entry for this workload, or None."""
+    return MEASURED_DRAM_BYTES_PER_ENTRY.get((variant, scale, ef, lines))
+
+
+def roofline_of(stats, K, hi: bool, k_lines: int, traffic_per_entry=None) -> dict:
+    """Roofline of the dominant kernel over K batches (SURVEY-style
+    algorithmic bytes: 8 B per covered adjacency entry for HI, 12 B for HB;
+    16 B per line for the structural kernel)."""
+    rec_ms = sum(s.recolor_ms for s in stats)
+    str_ms = sum(s.struct_ms for s in stats)
+    scanned = sum(s.slots_scanned for s in stats)
+    per_slot = 8 if hi else 12  # adjacency id + neighbour colour (+ priority)
+    peak, peak_kind = hbm_peak()
+    if rec_ms >= str_ms:
+        dom, dom_ms, alg = "recolor_kernel", rec_ms, per_slot * scanned
+    else:
+        dom, dom_ms, alg = "struct_kernel", str_ms, 16 * 2 * k_lines * K
+    achieved = alg / (dom_ms / 1e3) / 1e9
+    traffic = traffic_per_entry * scanned / K if traffic_per_entry and dom == "recolor_kernel" else None
+    out = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+           "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+           "algorithmic_bytes_per_launch": alg / K,
+           "entries_covered_per_launch": scanned / K,
+           "entries_read_per_launch": sum(s.slots_read for s in stats) / K,
+           "note": f"{per_slot} B per covered adjacency entry (id + neighbour colour"
+                   + ("" if hi else " + priority") + "), covered entries counted on the device"}
+    if traffic is not None:
+        # measured DRAM bytes of a launch over its duration, against the peak
+        out["dram_gbs"] = traffic / (dom_ms / K / 1e3) / 1e9
+        out["dram_frac"] = out["dram_gbs"] / peak
+    return out
+
+
+def measure_batches(ctx, dbat, k, W, K, stream):
+    """W untimed batches, then K timed ones (CUDA events on the library's
+    stream); returns (ms, per-batch stats)."""
+    import torch
+
+    for i in range(W):
+        ctx.apply_batch_device(dbat[i].data_ptr(), k)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = [ctx.apply_batch_device(dbat[W + i].data_ptr(), k) for i in range(K)]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), stats
 
 
 # ---------------------------------------------------------------------------
-# CPU baselines (checker code under oracle/, used only here as the baseline)
+# CPU baseline and oracle check (checker code under oracle/, used only here)
 # ---------------------------------------------------------------------------
 
-def cpu_baseline_oracle(args, w) -> dict:
+def oracle_first_batch(args, w, gpu_colors, gpu_stats) -> tuple[dict, dict]:
+    """Replays the first batch of the headline sequence (applied to the
+    initial graph) on the C oracle with every host thread, compares its
+    colours and step counts with the GPU's, and reports the same run as the
+    CPU baseline."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
 
     threads = os.cpu_count() or 1
     po.set_threads(threads)
+    t0 = time.perf_counter()
     g = po.Graph(w["n"])
     g.load_edges(w["a"], w["b"])
     g.set_colors(w["colors"])
-    ch = w["batches"][0][: args.cpu_sample]
+    load_s = time.perf_counter() - t0
+    ch = w["batches"][0]
     och = np.empty(len(ch), dtype=po.CHANGE_DTYPE)
     for f in ("node1", "node2", "inst"):
         och[f] = ch[f]
     t0 = time.perf_counter()
     rc, st = g.apply_batch(och, po.HI if args.variant == "hi" else po.HB, po.SNAPSHOT)
     dt = time.perf_counter() - t0
-    return {"value": len(och) / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": (f"first {len(och)} lines of batch 1 applied to the initial graph by the C "
-                       f"oracle (snapshot schedule, {threads} OpenMP threads): {dt:.2f} s, "
-                       f"{st.iterations} iterations")}
+    oc = g.colors()
+    diff = int(np.count_nonzero(oc != gpu_colors))
+    check = {
+        "batch": "first batch of the sequence, applied to the initial graph",
+        "lines": int(len(och)), "oracle_status": int(rc),
+        "colors_identical": diff == 0, "colors_differing": diff,
+        "iterations_gpu": int(gpu_stats.iterations), "iterations_oracle": int(st.iterations),
+        "frontier_total_equal": int(gpu_stats.frontier_total) == int(st.frontier_total),
+        "entries_covered_equal": int(gpu_stats.slots_scanned) == int(st.slots_scanned),
+        "max_color_gpu": int(gpu_colors.max()), "max_color_oracle": int(st.max_color),
+        "oracle_conflicts": int(g.conflicts()),
+    }
+    check["bit_exact"] = (diff == 0 and check["iterations_gpu"] == check["iterations_oracle"]
+                          and check["frontier_total_equal"] and check["entries_covered_equal"])
+    base = {"value": len(och) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"one full batch ({len(och)} lines, the first of the sequence) applied to the "
+                       f"initial graph by the C oracle (snapshot schedule, {threads} OpenMP threads): "
+                       f"{dt:.1f} s, {st.iterations} iterations; graph load {load_s:.1f} s not timed")}
+    return check, base
 
 
-def run_reference(args, dist: Dist) -> dict:
-    """The reference's own kernel bodies, run serially on the host (oracle/_ref)."""
+def run_reference(args, dist) -> dict:
+    """The reference's own kernel bodies on the host cores (oracle/_ref),
+    every kernel launched on all host threads.  The inputs come from the
+    generators compiled into the checker library, so this arm never loads
+    libdyncolor.so.  Only steps whose recolouring converged count."""
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_hi" if args.variant == "hi" else "ref_hb")
     if not os.path.exists(exe):
         return {"impl": "reference", "unavailable": "oracle/_ref harness not built (reference sources absent at build time)"}
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
 
+    threads = os.cpu_count() or 1
     nb = args.warmup + args.steps
-    w = build_workload(args, nb)
+    w = build_workload(args, nb, gen=_CheckerGen())
     d = tempfile.mkdtemp()
     try:
         np.stack([w["a"], w["b"]], 1).astype(np.int32).tofile(os.path.join(d, "g.bin"))
@@ -331,29 +436,32 @@ def run_reference(args, dist: Dist) -> dict:
         out = os.path.join(d, "o.txt")
         subprocess.run([exe, "bench", os.path.join(d, "g.bin"), str(w["n"]), str(len(w["a"])),
                         os.path.join(d, "c.bin"), ",".join(files), out, str(args.ref_iter_cap),
-                        str(args.ref_step_budget_ms)],
+                        str(args.ref_step_budget_ms), str(args.ref_max_fail), str(threads)],
                        check=True, stdout=subprocess.DEVNULL)
         rows = [line.split() for line in open(out)]
     finally:
         shutil.rmtree(d, ignore_errors=True)
-    timed = rows[args.warmup:]
-    ms = sum(float(r[5]) for r in timed)
-    its = [int(r[1]) for r in timed]
-    capped = sum(1 for r in timed if r[3] != "0")
-    lines = args.ref_sample * len(timed)
+    its = [int(r[1]) for r in rows]
+    conv = [r for r in rows[args.warmup:] if r[3] == "0"]
+    how = (f"first {args.ref_sample} lines of each batch, each applied to the initial graph by the "
+           f"reference's own kernel bodies, every kernel launched on {threads} host threads; step budget "
+           f"{args.ref_step_budget_ms / 1e3:.0f} s or {args.ref_iter_cap} iterations")
+    if not conv:
+        return {"impl": "reference", "unavailable": (
+            f"the reference's recolouring converged on none of the {len(rows)} steps run ({how}; loop "
+            f"iterations {its}; stopped after {args.ref_max_fail} unconverged steps in a row): its 32-bit "
+            f"saturation masks are exact only for colours <= 30 and this graph starts with "
+            f"{int(w['colors'].max()) + 1} colours")}
+    ms = sum(float(r[5]) for r in conv)
+    lines = args.ref_sample * len(conv)
     value = lines / (ms / 1e3)
-    sample = (f"first {args.ref_sample} lines of each of {len(timed)} batches, each applied to the "
-              f"initial graph by the reference's own kernel bodies run serially on 1 host core "
-              f"(loop iterations {its}; {capped} of {len(timed)} steps stopped at the "
-              f"{args.ref_iter_cap}-iteration cap or the {args.ref_step_budget_ms / 1e3:.0f} s step budget "
-              f"before the recolouring converged, so the value overstates the reference; the "
-              f"reference's 32-bit masks are exact only for colours <= 30)")
+    sample = f"{how}; {len(conv)} timed steps converged and count (loop iterations of all steps {its})"
     return {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": dist.world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / len(timed),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / len(conv),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic", "config": config(args, w),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -361,6 +469,84 @@ def run_reference(args, dist: Dist) -> dict:
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+
+def sub_result(name, desc, ctx_args, n, a, b, colors, batches, W, K, hi, dev, stream, graph_desc,
+               traffic=None) -> dict:
+    """One further configuration: fresh context, W untimed and K timed
+    batches, device time, roofline, and a properness check."""
+    import torch
+
+    import dyncolor_b200 as dc
+
+    ctx = dc.Context(variant=dc.HI if hi else dc.HB, device=dev, stream=stream.cuda_stream, **ctx_args)
+    ctx.load_edges(n, a, b)
+    ctx.set_colors(colors)
+    k = len(batches[0])
+    dbat = [torch.from_numpy(np.ascontiguousarray(x).view(np.int32).reshape(-1, 3)).to(f"cuda:{dev}")
+            for x in batches[: W + K]]
+    ms, stats = measure_batches(ctx, dbat, k, W, K, stream)
+    conflicts = ctx.validate()
+    ctx.close()
+    del dbat
+    return {
+        "name": name, "workload": desc, "graph": graph_desc, "variant": "HI" if hi else "HB",
+        "batch_lines": k, "warmup": W, "steps": K,
+        "value": K * k / (ms / 1e3), "unit": UNIT, "ms_per_batch": ms / K,
+        "iterations_per_batch": [int(s.iterations) for s in stats],
+        "recolor_ms_per_batch": sum(s.recolor_ms for s in stats) / K,
+        "struct_ms_per_batch": sum(s.struct_ms for s in stats) / K,
+        "roofline": roofline_of(stats, K, hi, k, traffic),
+        "max_color": int(max(s.max_color for s in stats)),
+        "conflicts_after": int(conflicts),
+    }
+
+
+def run_further_configs(args, w, dev, stream) -> list:
+    """The other single-graph configurations: the headline graph with 100 k
+    and 10 M-line batches and with the HB variant, and the skewed-degree
+    Chung-Lu graph (both variants)."""
+    import dyncolor_b200 as dc
+
+    out = []
+    n, a, b, col = w["n"], w["a"], w["b"], w["colors"]
+    gd = {"vertices": int(n), "edges": int(len(a)), "generator": "R-MAT a=0.57 b=c=0.19",
+          "initial_colors": int(col.max()) + 1}
+    ctx_args = dict(unit_slots=args.unit_slots, blocks_per_sm=args.blocks_per_sm,
+                    heavy_min_live=args.heavy_min_live)
+    for lines, W, K in ((100_000, 2, 5), (10_000_000, 1, 2)):
+        es = dc.EdgeSet(n, a, b)
+        bs = [es.sample_batch(lines // 2, lines - lines // 2, mode=dc.INS_RMAT, scale=args.scale,
+                              seed=args.seed * 7000 + lines // 1000 + i) for i in range(W + K)]
+        del es
+        out.append(sub_result(f"rmat{args.scale}_b{lines}_hi",
+                              f"rmat{args.scale}-ef{args.edgefactor}, batches of {lines} lines in sequence "
+                              f"(50/50, R-MAT endpoints)", ctx_args, n, a, b, col, bs, W, K, True, dev, stream,
+                              gd, load_traffic("hi", args.scale, args.edgefactor, lines)))
+    out.append(sub_result(f"rmat{args.scale}_b{args.batch}_hb",
+                          f"rmat{args.scale}-ef{args.edgefactor}, batches of {args.batch} lines in sequence "
+                          f"(the headline batches), variant HB", ctx_args, n, a, b, col, w["batches"], 1, 2, False,
+                          dev, stream, gd, load_traffic("hb", args.scale, args.edgefactor, args.batch)))
+    # skewed degrees: Chung-Lu, exponent 2.1, 4 M vertices, average degree 24
+    cn = args.cl_vertices
+    t0 = time.time()
+    ca, cb = dc.chung_lu(cn, 2.1, 24.0, args.cl_max_deg, seed=args.seed + 3)
+    ca, cb = dc.dedup(cn, ca, cb)
+    ccol = dc.greedy_color(cn, ca, cb)
+    deg = np.bincount(ca, minlength=cn) + np.bincount(cb, minlength=cn)
+    es = dc.EdgeSet(cn, ca, cb)
+    kd = int(0.3 * args.batch)
+    cbs = [es.sample_batch(kd, args.batch - kd, mode=dc.INS_DEGREE, seed=args.seed * 9000 + i) for i in range(4)]
+    del es
+    cgd = {"vertices": int(cn), "edges": int(len(ca)), "generator": "Chung-Lu gamma=2.1 avg degree 24",
+           "max_degree": int(deg.max()), "initial_colors": int(ccol.max()) + 1,
+           "gen_s": round(time.time() - t0, 1)}
+    for hi, W, K in ((True, 1, 3), (False, 1, 2)):
+        out.append(sub_result(f"chunglu_{cn}_b{args.batch}_{'hi' if hi else 'hb'}",
+                              f"Chung-Lu (gamma 2.1) {cn} vertices, batches of {args.batch} lines in sequence "
+                              f"(70% insertions with one endpoint drawn by degree, 30% deletions)",
+                              ctx_args, cn, ca, cb, ccol, cbs, W, K, hi, dev, stream, cgd))
+    return out
+
 
 def run_ours(args, dist: Dist):
     import torch
@@ -384,17 +570,20 @@ def run_ours(args, dist: Dist):
     dbat = [torch.from_numpy(np.ascontiguousarray(x).view(np.int32).reshape(-1, 3)).to(f"cuda:{dev}")
             for x in w["batches"][: W + K]]
     torch.cuda.synchronize()
-    for i in range(W):
+    # the first warm-up batch's colours are kept for the oracle check
+    first_stats = ctx.apply_batch_device(dbat[0].data_ptr(), k)
+    first_colors = ctx.colors().copy() if dist.rank == 0 else None
+    for i in range(1, W):
         ctx.apply_batch_device(dbat[i].data_ptr(), k)
     torch.cuda.synchronize()
     dist.barrier()
     clocks = ClockSampler(dev)
     clocks.start()
     time.sleep(0.3)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     stats = []
     for i in range(K):
@@ -421,23 +610,10 @@ def run_ours(args, dist: Dist):
     torch.cuda.synchronize()
     e2e_s = dist.max(time.perf_counter() - t0)
     conflicts = ctx.validate()
+    ctx.close()
     del dbat
-    # roofline of the dominant kernel
-    rec_ms = sum(s.recolor_ms for s in stats)
-    str_ms = sum(s.struct_ms for s in stats)
-    scanned = sum(s.slots_scanned for s in stats)
-    per_slot = 8 if variant == dc.HI else 12  # adjacency id + neighbour colour (+ priority)
-    peak, peak_kind = hbm_peak()
-    if rec_ms >= str_ms:
-        dom, dom_ms, alg = "recolor_kernel", rec_ms, per_slot * scanned
-    else:
-        dom, dom_ms = "struct_kernel", str_ms
-        alg = 16 * 2 * k * K
-    achieved = alg / (dom_ms / 1e3) / 1e9
-    traffic = None
-    tr = load_traffic(args)
-    if tr and dom == "recolor_kernel":
-        traffic = tr * scanned / K  # per launch, like `achieved`
+    torch.cuda.empty_cache()
+    roof = roofline_of(stats, K, variant == dc.HI, k, load_traffic(args.variant, args.scale, args.edgefactor, k))
     out = {
         "metric": METRIC,
         "value": value,
@@ -457,32 +633,27 @@ def run_ours(args, dist: Dist):
         # per batch: structural + recolour launches, and the three heavy-row
         # index kernels when the batch uses the index (lines * 32 >= n)
         "gpu_launches": (5 if args.heavy_min_live >= 0 and k * 32 >= int(w["n"]) else 2) * K,
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg / K,
-                     "entries_covered_per_launch": scanned / K,
-                     "entries_read_per_launch": sum(s.slots_read for s in stats) / K,
-                     "note": f"{per_slot} B per scanned adjacency entry (id + neighbour colour"
-                             + (" + priority" if variant == dc.HB else "") + ")"},
+        "roofline": roof,
         "clocks": clk,
         "detail": {
             "iterations_per_batch": [int(s.iterations) for s in stats],
-            "struct_ms_per_batch": str_ms / K,
-            "recolor_ms_per_batch": rec_ms / K,
-            "phase_ms_per_batch": {k: round(sum(s.phase_ms[i] for s in stats) / K, 3)
-                                   for i, k in enumerate(("seeding", "find_eligible", "mex", "commit"))},
-            "slots_scanned_per_batch": scanned / K,
+            "struct_ms_per_batch": sum(s.struct_ms for s in stats) / K,
+            "recolor_ms_per_batch": sum(s.recolor_ms for s in stats) / K,
+            "phase_ms_per_batch": {nm: round(sum(s.phase_ms[i] for s in stats) / K, 3)
+                                   for i, nm in enumerate(("seeding", "find_eligible", "mex", "commit"))},
+            "slots_scanned_per_batch": sum(s.slots_scanned for s in stats) / K,
             "slots_read_per_batch": sum(s.slots_read for s in stats) / K,
-            "pairs_per_batch": sum(s.pairs for s in stats) / K,
             "max_color": int(max(s.max_color for s in stats)),
             "conflicts_after": int(conflicts),
             "workload_gen_s": round(w["gen_s"], 1),
             "load_s": round(load_s, 2),
         },
     }
-    ctx.close()
-    return out, w
+    if dist.world == 1 and not args.no_further_configs:
+        t0 = time.time()
+        out["detail"]["configs"] = run_further_configs(args, w, dev, stream)
+        out["detail"]["configs_s"] = round(time.time() - t0, 1)
+    return out, w, first_colors, first_stats
 
 
 # ---------------------------------------------------------------------------
@@ -777,10 +948,12 @@ def main():
         return
     dist = Dist(args.gpus)
     try:
-        out, w = run_ours(args, dist)
+        out, w, first_colors, first_stats = run_ours(args, dist)
         if dist.rank == 0:
             if dist.world == 1 and not args.no_cpu_baseline:
-                out["cpu_baseline"] = cpu_baseline_oracle(args, w)
+                check, base = oracle_first_batch(args, w, first_colors, first_stats)
+                out["detail"]["oracle_checked"] = check
+                out["cpu_baseline"] = base
             print(json.dumps(out), flush=True)
     finally:
         dist.close()

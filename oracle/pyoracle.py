@@ -73,6 +73,22 @@ def lib():
         L.orc_greedy_id_order.argtypes = [P]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_instrument.argtypes = [C.c_int]
+        # seeded workload generators (dc_gen.cpp compiled into this library)
+        L.dcg_rmat.argtypes = [C.c_int32, C.c_int32, C.c_int64, C.c_double, C.c_double, C.c_double,
+                               C.c_uint64, P, P]
+        L.dcg_chung_lu.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double, C.c_uint64, P, P,
+                                   C.c_int64]
+        L.dcg_chung_lu.restype = C.c_int64
+        L.dcg_dedup.argtypes = [C.c_int32, P, P, C.c_int64]
+        L.dcg_dedup.restype = C.c_int64
+        L.dcg_greedy_color.argtypes = [C.c_int32, P, P, C.c_int64, P]
+        L.dcg_edgeset_create.argtypes = [C.c_int32, P, P, C.c_int64]
+        L.dcg_edgeset_create.restype = P
+        L.dcg_edgeset_destroy.argtypes = [P]
+        L.dcg_edgeset_destroy.restype = None
+        L.dcg_edgeset_sample_batch.argtypes = [P, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
+                                               C.c_double, C.c_double, C.c_double, C.c_uint64, P]
+        L.dcg_edgeset_sample_batch.restype = C.c_int64
         _lib = L
     return _lib
 
@@ -152,6 +168,77 @@ class Graph:
 
 def set_threads(n: int) -> None:
     lib().orc_set_threads(int(n))
+
+
+# ---------------------------------------------------------------------------
+# workload generators (the product's dc_gen.cpp, compiled into liboracle.so,
+# so a checker-side process can build the benchmark inputs without loading
+# libdyncolor.so; same seeds give the same graphs and batches)
+# ---------------------------------------------------------------------------
+
+INS_UNIFORM, INS_RMAT, INS_DEGREE = 0, 1, 2
+
+
+def gen_rmat(scale: int, m: int, seed: int = 1, a=0.57, b=0.19, c=0.19):
+    n = 1 << scale
+    xa = np.empty(m, dtype=np.int32)
+    xb = np.empty(m, dtype=np.int32)
+    if lib().dcg_rmat(scale, n, m, a, b, c, seed, _ptr(xa), _ptr(xb)) != OK:
+        raise RuntimeError("dcg_rmat")
+    return xa, xb
+
+
+def gen_chung_lu(n: int, gamma: float, avg_deg: float, max_deg: float, seed: int = 1):
+    cap = int(round(n * avg_deg / 2)) + 1
+    xa = np.empty(cap, dtype=np.int32)
+    xb = np.empty(cap, dtype=np.int32)
+    m = lib().dcg_chung_lu(n, gamma, avg_deg, max_deg, seed, _ptr(xa), _ptr(xb), cap)
+    if m < 0:
+        raise RuntimeError("dcg_chung_lu")
+    return xa[:m].copy(), xb[:m].copy()
+
+
+def gen_dedup(n: int, a, b):
+    a = np.array(a, dtype=np.int32, copy=True)
+    b = np.array(b, dtype=np.int32, copy=True)
+    m = lib().dcg_dedup(n, _ptr(a), _ptr(b), len(a))
+    if m < 0:
+        raise RuntimeError("dcg_dedup")
+    return a[:m].copy(), b[:m].copy()
+
+
+def gen_greedy_color(n: int, a, b) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.int32)
+    b = np.ascontiguousarray(b, dtype=np.int32)
+    out = np.zeros(n, dtype=np.int32)
+    if lib().dcg_greedy_color(n, _ptr(a), _ptr(b), len(a), _ptr(out)) != OK:
+        raise RuntimeError("dcg_greedy_color")
+    return out
+
+
+class GenEdgeSet:
+    """Edge set that draws update batches (dcg_edgeset)."""
+
+    def __init__(self, n: int, a, b):
+        a = np.ascontiguousarray(a, dtype=np.int32)
+        b = np.ascontiguousarray(b, dtype=np.int32)
+        self._h = lib().dcg_edgeset_create(n, _ptr(a), _ptr(b), len(a))
+        if not self._h:
+            raise MemoryError("dcg_edgeset_create")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().dcg_edgeset_destroy(h)
+            self._h = None
+
+    def sample_batch(self, k_del: int, k_ins: int, mode: int = INS_UNIFORM, scale: int = 0, seed: int = 1,
+                     a=0.57, b=0.19, c=0.19) -> np.ndarray:
+        out = np.empty(k_del + k_ins, dtype=CHANGE_DTYPE)
+        w = lib().dcg_edgeset_sample_batch(self._h, k_del, k_ins, mode, scale, a, b, c, seed, _ptr(out))
+        if w < 0:
+            raise RuntimeError("dcg_edgeset_sample_batch")
+        return out[:w]
 
 
 # ---------------------------------------------------------------------------

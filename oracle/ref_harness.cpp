@@ -27,10 +27,15 @@
  * usage: ref_{hi,hb} serial|snapshot graph nodes edges prevColor changes out [iter_cap]
  * out: "iterations <n> status <0|4>\n" then one colour per line.
  *
- * Timing mode (serial schedule, for the CPU baseline of the benchmark):
- *   ref_{hi,hb} bench graph.bin nodes edges colors.bin ch1[,ch2,...] out [iter_cap [budget_ms]]
- *   (a step stops at iter_cap loop iterations or once its timed work passes
- *   budget_ms, with status 4, so a timing run ends in bounded time)
+ * Timing mode (for the reference arm of the benchmark):
+ *   ref_{hi,hb} bench graph.bin nodes edges colors.bin ch1[,ch2,...] out
+ *               [iter_cap [budget_ms [max_fail [threads]]]]
+ *   Every kernel is launched on `threads` host threads (default: all of
+ *   OpenMP's): each thread runs the kernel's grid-stride loop over its share
+ *   of the items, racing on the shared arrays as the reference's GPU threads
+ *   do.  A step stops at iter_cap loop iterations or once its timed work
+ *   passes budget_ms, with status 4, so a timing run ends in bounded time;
+ *   after max_fail such steps in a row (default: never) the rest are skipped.
  * graph.bin holds int32 pairs (a0 b0 a1 b1 ...) turned into the adjacency the
  * way read_graphEdges does; colors.bin holds one int32 per vertex.  Every
  * change file is one step applied to the initial graph and colouring (the
@@ -39,6 +44,8 @@
  * between them is not timed); out gets one line per step:
  * "iterations <n> status <s> time_ms <t>".
  */
+#include <omp.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -99,6 +106,23 @@ bool snapshot_step(State& S, int nitems, F run_item) {
   return true;
 }
 
+// Runs kernel body f as a launch of `threads` host threads (see the shim).
+template <class F>
+void launch(int threads, F f) {
+  if (threads <= 1) {
+    f();
+    return;
+  }
+  blockDim.x = (unsigned)threads;
+#pragma omp parallel num_threads(threads)
+  {
+    threadIdx.x = (unsigned)omp_get_thread_num();
+    f();
+    threadIdx.x = 0;
+  }
+  blockDim.x = 1;
+}
+
 int compact(const State& S, std::vector<int>& list) {
   int c = 0;
   for (int v = 0; v < S.n; ++v)
@@ -128,7 +152,7 @@ struct StepResult {
 // One update batch as the reference driver applies it
 // (HI/Color_main.cu:62-202, HB/Color_main.cu:71-224).
 StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long iter_cap,
-                    double budget_ms = 0.0) {
+                    double budget_ms = 0.0, int threads = 1) {
   using clk = std::chrono::steady_clock;
   StepResult R;
   const int nodes = G.nodes;
@@ -168,7 +192,7 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
   bool ok = true;
 
   if (!allChange_Del.empty())
-    deleteEdgeFromAdj(allChange_Del.data(), (int)allChange_Del.size(), adj, trk);
+    launch(threads, [&] { deleteEdgeFromAdj(allChange_Del.data(), (int)allChange_Del.size(), adj, trk); });
 
 #ifdef REF_HI
   if (!allChange_Del.empty()) {
@@ -178,8 +202,10 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
                    S.affected.data(), &S.change, W);
       });
     } else {
-      deleteEdge(allChange_Del.data(), S.color.data(), S.prev.data(), (int)allChange_Del.size(),
-                 adj, trk, S.affected.data(), &S.change, W);
+      launch(threads, [&] {
+        deleteEdge(allChange_Del.data(), S.color.data(), S.prev.data(), (int)allChange_Del.size(), adj, trk,
+                   S.affected.data(), &S.change, W);
+      });
     }
   }
   if (!allChange_Ins.empty()) {
@@ -189,8 +215,10 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
                 S.affected.data(), &S.change, W);
       });
     } else {
-      insEdge(allChange_Ins.data(), S.color.data(), S.prev.data(), (int)allChange_Ins.size(), adj,
-              trk, S.affected.data(), &S.change, W);
+      launch(threads, [&] {
+        insEdge(allChange_Ins.data(), S.color.data(), S.prev.data(), (int)allChange_Ins.size(), adj, trk,
+                S.affected.data(), &S.change, W);
+      });
     }
   }
 #else
@@ -211,8 +239,10 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
                       prop);
     });
   } else if (!allChange.empty()) {
-    processChangeEdge(allChange.data(), S.color.data(), (int)allChange.size(), adj, trk,
-                      S.affected.data(), &S.change, prop);
+    launch(threads, [&] {
+      processChangeEdge(allChange.data(), S.color.data(), (int)allChange.size(), adj, trk, S.affected.data(),
+                        &S.change, prop);
+    });
   }
 #endif
 
@@ -228,13 +258,13 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
     ++it;
     S.change = 0;
     std::fill(S.affected.begin(), S.affected.end(), 0);
+    launch(threads, [&] {
 #ifdef REF_HI
-    findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.prev.data(), S.color.data(),
-                          &counter);
+      findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.prev.data(), S.color.data(), &counter);
 #else
-    findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.color.data(), &counter,
-                          prop);
+      findEligibleNeighbors(list.data(), adj, trk, S.affected.data(), S.color.data(), &counter, prop);
 #endif
+    });
     counter = compact(S, list);
     std::fill(S.affected.begin(), S.affected.end(), 0);
     if (snapshot) {
@@ -248,13 +278,14 @@ StepResult run_step(Graph& G, State& S, const char* changes, bool snapshot, long
 #endif
       });
     } else {
+      launch(threads, [&] {
 #ifdef REF_HI
-      recolorNeighbor(list.data(), S.color.data(), S.prev.data(), adj, trk, S.affected.data(),
-                      &counter, &S.change, W);
+        recolorNeighbor(list.data(), S.color.data(), S.prev.data(), adj, trk, S.affected.data(), &counter,
+                        &S.change, W);
 #else
-      recolorNeighbor(list.data(), S.color.data(), adj, trk, S.affected.data(), &counter,
-                      &S.change, prop);
+        recolorNeighbor(list.data(), S.color.data(), adj, trk, S.affected.data(), &counter, &S.change, prop);
 #endif
+      });
     }
   }
   R.ms += std::chrono::duration<double, std::milli>(clk::now() - t0).count();
@@ -277,6 +308,8 @@ int main(int argc, char* argv[]) {
   const int nodes = std::atoi(argv[3]);
   const long iter_cap = argc > 8 ? std::atol(argv[8]) : 100000;
   const double budget_ms = argc > 9 ? std::atof(argv[9]) : 0.0;  // bench mode: per-step time budget
+  const int max_fail = argc > 10 ? std::atoi(argv[10]) : 0;       // bench mode: stop after this many
+  const int threads = argc > 11 ? std::atoi(argv[11]) : omp_get_max_threads();
   Graph G;
   G.nodes = nodes;
   G.adj.resize(nodes);
@@ -340,6 +373,7 @@ int main(int argc, char* argv[]) {
 #endif
   std::string list = argv[6];
   size_t pos = 0;
+  int fails = 0;
   while (pos <= list.size()) {
     size_t comma = list.find(',', pos);
     if (comma == std::string::npos) comma = list.size();
@@ -356,14 +390,16 @@ int main(int argc, char* argv[]) {
       }
       std::fclose(cf);
     }
-    const StepResult R = run_step(G, S, file.c_str(), false, iter_cap, budget_ms);
-    std::fprintf(f, "iterations %ld status %d time_ms %.3f\n", R.iterations, R.status, R.ms);
+    const StepResult R = run_step(G, S, file.c_str(), false, iter_cap, budget_ms, threads);
+    std::fprintf(f, "iterations %ld status %d time_ms %.3f threads %d\n", R.iterations, R.status, R.ms, threads);
     std::fflush(f);
+    fails = R.status != 0 ? fails + 1 : 0;
     for (auto it = sizes.rbegin(); it != sizes.rend(); ++it) G.adj[it->first].resize(it->second);
     S = S0;
 #ifndef REF_HI
     G.prop = prop0;
 #endif
+    if (max_fail > 0 && fails >= max_fail) break;
   }
   std::fclose(f);
   return 0;

@@ -1,5 +1,8 @@
 """The CPU oracle against the reference's own code (golden vectors made by
 oracle/_ref from the reference sources) and against its known answers."""
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -109,3 +112,49 @@ def test_oracle_matches_reference_code_live():
                 it, status, rcol = po.run_ref(v, sch, a, b, col, ch, iter_cap=2000)
                 assert (it, status) == (st.iterations, st.status)
                 assert np.array_equal(rcol, g.colors())
+
+
+def test_checker_generators_match_the_product_generators():
+    """The generators compiled into liboracle.so (used by the benchmark's
+    reference arm, which must not load libdyncolor.so) give the same graphs,
+    colourings and batches as the product's."""
+    import dyncolor_b200 as dc
+
+    n = 1 << 12
+    a1, b1 = po.gen_dedup(n, *po.gen_rmat(12, 16 * n, seed=3))
+    a2, b2 = dc.dedup(n, *dc.rmat(12, 16 * n, seed=3))
+    assert np.array_equal(a1, a2) and np.array_equal(b1, b2)
+    assert np.array_equal(po.gen_greedy_color(n, a1, b1), dc.greedy_color(n, a2, b2))
+    x1 = po.GenEdgeSet(n, a1, b1).sample_batch(300, 300, mode=po.INS_RMAT, scale=12, seed=5)
+    x2 = dc.EdgeSet(n, a2, b2).sample_batch(300, 300, mode=dc.INS_RMAT, scale=12, seed=5)
+    assert np.array_equal(x1.view(np.int32), x2.view(np.int32))
+    c1 = po.gen_chung_lu(5000, 2.1, 24.0, 250.0, seed=2)
+    c2 = dc.chung_lu(5000, 2.1, 24.0, 250.0, seed=2)
+    assert np.array_equal(c1[0], c2[0]) and np.array_equal(c1[1], c2[1])
+
+
+def test_reference_arm_loads_only_checker_code(tmp_path):
+    """bench.py --impl reference builds its inputs with the checker's
+    generators and runs the reference's own kernel bodies: libdyncolor.so is
+    never mapped into that process."""
+    import subprocess
+    import sys
+
+    if not po.ref_available():
+        pytest.skip("reference harness not built")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    probe = tmp_path / "probe.py"
+    probe.write_text(
+        "import json, runpy, sys\n"
+        f"sys.argv = ['bench.py', '--impl', 'reference', '--scale', '12', '--batch', '2000', "
+        "'--steps', '2', '--warmup', '1', '--ref-sample', '200']\n"
+        f"sys.path.insert(0, {root!r})\n"
+        "import bench\n"
+        "bench.main()\n"
+        "maps = open('/proc/self/maps').read()\n"
+        "print(json.dumps({'dyncolor': 'libdyncolor' in maps, 'oracle': 'liboracle' in maps}))\n")
+    r = subprocess.run([sys.executable, str(probe)], capture_output=True, text=True, cwd=root, timeout=600)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert lines[0]["impl"] == "reference" and lines[0]["value"] > 0
+    assert lines[1] == {"dyncolor": False, "oracle": True}
