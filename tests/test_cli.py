@@ -1,0 +1,77 @@
+"""The `dyncolor` command (dyncolor_b200/dyncolor, built from
+dyncolor_b200/csrc/dc_cli.cpp): the reference drivers' argv
+(HI/Color_main.cu:21-37) and text files (HI/all_structure_undir.cuh:78-183),
+run on the reference's sample fixture and on golden cases written out in the
+reference's formats, compared with the colours the reference's own kernel
+code gives under the snapshot schedule (tests/golden)."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import dyncolor_b200 as dc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "dyncolor_b200", "dyncolor")
+
+
+def _write_case(d, c, newline_at_end=False):
+    """Graph "a b w", colour "node color" and change "a b w inst" lines; the
+    last line of the graph file has no newline, like the reference's own
+    graph.txt."""
+    g, col, ch = (os.path.join(d, x) for x in ("graph.txt", "prevColor.txt", "cE.txt"))
+    lines = [f"{x} {y} 1" for x, y in zip(c["a"].tolist(), c["b"].tolist())]
+    with open(g, "w") as f:
+        f.write("\n".join(lines) + ("\n" if newline_at_end else ""))
+    with open(col, "w") as f:
+        f.write("".join(f"{v} {x}\n" for v, x in enumerate(c["colors"].tolist())))
+    with open(ch, "w") as f:
+        f.write("".join(f"{x} {y} 1 {t}\n" for x, y, t in c["changes"].tolist()))
+    return g, col, ch
+
+
+def _run(args, cwd):
+    return subprocess.run([CLI] + [str(x) for x in args], capture_output=True, text=True, cwd=cwd, timeout=300)
+
+
+def test_cli_rejects_bad_arguments_before_touching_a_device(tmp_path):
+    assert os.path.exists(CLI), "dyncolor command not built (make -C dyncolor_b200/csrc)"
+    assert _run([], tmp_path).returncode == 2
+    assert _run(["g", "10", "19", "c", "x", "--variant", "xx"], tmp_path).returncode == 2
+    (tmp_path / "c.txt").write_text("0 1\n11 2\n")  # vertex 11 of 10
+    (tmp_path / "g.txt").write_text("0 1 1\n")
+    (tmp_path / "x.txt").write_text("")
+    r = _run(["g.txt", "10", "1", "c.txt", "x.txt"], tmp_path)
+    assert r.returncode == 2 and "outside" in r.stderr
+    assert _run(["missing.txt", "10", "1", "c.txt", "x.txt"], tmp_path).returncode == 2
+
+
+@pytest.mark.gpu
+def test_cli_on_reference_fixture_and_golden_cases(golden, tmp_path):
+    cases = [c for c in golden if c["name"].startswith("sample")] + \
+            [c for c in golden if not c["name"].startswith("sample")][:12]
+    bad = []
+    for i, c in enumerate(cases):
+        d = tmp_path / f"case{i}"
+        d.mkdir()
+        g, col, ch = _write_case(str(d), c, newline_at_end=bool(i % 2))
+        out = str(d / "out.txt")
+        variant = "hb" if int(c["variant"][0]) == dc.HB else "hi"
+        n = int(c["n"][0])
+        r = _run([g, n, len(c["a"]), col, ch, "--variant", variant, "--out", out], str(d))
+        want_it, want_status = c["snapshot_iters"]
+        if want_status != 0:
+            continue  # capped runs are covered by the library tests
+        if r.returncode != 0:
+            bad.append((c["name"], r.returncode, r.stderr[-300:]))
+            continue
+        got = np.zeros(n, np.int32)
+        for line in open(out):
+            v, x = line.split()
+            got[int(v)] = int(x)
+        its = [int(x.split("(")[1].split()[0]) for x in r.stdout.splitlines() if "affected neighbors" in x][0]
+        if not np.array_equal(got, c["snapshot_colors"]) or its != int(want_it):
+            bad.append((c["name"], got.tolist(), c["snapshot_colors"].tolist(), its, int(want_it)))
+        assert "highest color id used: %d" % int(got.max()) in r.stdout
+    assert not bad, bad[:4]
