@@ -34,6 +34,7 @@ LIB_PATH = os.path.join(HERE, "libdyncolor.so")
 HI, HB = 0, 1
 OK, E_INVAL, E_NOMEM, E_CUDA, E_ITER_LIMIT, E_STATE, E_TIMEOUT, E_INTERNAL = range(8)
 INS_UNIFORM, INS_RMAT, INS_DEGREE = 0, 1, 2
+ORDER_ID, ORDER_LDF = 0, 1
 
 CHANGE_DTYPE = np.dtype([("node1", "<i4"), ("node2", "<i4"), ("inst", "<i4")])
 
@@ -116,6 +117,7 @@ def lib() -> C.CDLL:
     L.dc_graph_load_edges.argtypes = [P, C.c_int32, P, P, C.c_int64]
     L.dc_colors_set.argtypes = [P, P, C.c_int32]
     L.dc_colors_init_greedy.argtypes = [P]
+    L.dc_colors_init.argtypes = [P, C.c_int32]
     L.dc_apply_batch.argtypes = [P, P, C.c_int64, C.POINTER(Stats)]
     L.dc_apply_batch_device.argtypes = [P, P, C.c_int64, C.POINTER(Stats)]
     L.dc_colors_read.argtypes = [P, P, C.c_int32]
@@ -241,6 +243,12 @@ class Context:
     def init_greedy_colors(self):
         """Greedy lowest-free colouring in vertex-id order of the current graph."""
         self._check(lib().dc_colors_init_greedy(self._h), "dc_colors_init_greedy")
+
+    def init_colors(self, order: int = ORDER_ID):
+        """Greedy lowest-free colouring of the current graph in the given
+        order (ORDER_ID: vertex ids; ORDER_LDF: largest live degree first),
+        computed on the device."""
+        self._check(lib().dc_colors_init(self._h, int(order)), "dc_colors_init")
 
     def apply_batch(self, changes, check: bool = True) -> Stats:
         ch = np.ascontiguousarray(changes, dtype=CHANGE_DTYPE)

@@ -793,77 +793,65 @@ dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n) {
   return DC_OK;
 }
 
-dc_status dc_colors_init_greedy(dc_ctx* ctx) {
+dc_status dc_colors_init(dc_ctx* ctx, int32_t order) {
   if (dc_status g_ = gate(ctx)) return g_;
+  if (order != DC_ORDER_ID && order != DC_ORDER_LDF) return fail(ctx, DC_E_INVAL, "unknown colouring order");
   cudaSetDevice(ctx->device);
   cudaGetLastError();  // start from a clean error state
-  const int n = ctx->n;
-  std::vector<int> live((size_t)std::max(n, 1)), col((size_t)std::max(n, 1), 0);
-  if (n > 0) DC_CK(cudaMemcpyAsync(live.data(), ctx->live, (size_t)n * 4, cudaMemcpyDeviceToHost, ctx->stream));
-  DC_CK(cudaStreamSynchronize(ctx->stream));
-  std::vector<long long> pre((size_t)n + 1, 0);
-  int maxlive = 0;
-  for (int v = 0; v < n; ++v) {
-    pre[(size_t)v + 1] = pre[(size_t)v] + live[(size_t)v];
-    maxlive = std::max(maxlive, live[(size_t)v]);
-  }
-  // rows come back in vertex order, a chunk of rows at a time
-  const long long kRows = 1ll << 20;
-  const long long stage_cap = std::max<long long>(1ll << 24, maxlive);
-  long long* dpre = nullptr;
-  int* dstage = nullptr;
   dc_status s;
-  if ((s = dalloc(ctx, &dpre, kRows + 1, "greedy chunk offsets")) != DC_OK) return s;
-  if ((s = dalloc(ctx, &dstage, stage_cap, "greedy staging")) != DC_OK) {
-    dfree(ctx, &dpre);
+  if ((s = ensure_recolor_scratch(ctx)) != DC_OK) return s;
+  const long long n = std::max(ctx->n, 1);
+  int* prio = nullptr;
+  int* pred = nullptr;
+  unsigned long long* cp = nullptr;
+  auto drop = [&]() {
+    dfree(ctx, &prio);
+    dfree(ctx, &pred);
+    dfree(ctx, &cp);
+  };
+  if ((s = dalloc(ctx, &prio, n, "colouring priorities")) != DC_OK ||
+      (s = dalloc(ctx, &pred, n, "colouring predecessor counts")) != DC_OK ||
+      (s = dalloc(ctx, &cp, n, "colouring packed words")) != DC_OK) {
+    drop();
     return s;
   }
-  std::vector<long long> prerel((size_t)kRows + 1);
-  std::vector<int> rows((size_t)stage_cap);
-  std::vector<unsigned> stamp((size_t)maxlive + 2, 0u);
-  unsigned gen = 0;
-  const GraphDev gd = graph_dev(ctx);
-  cudaError_t e = cudaSuccess;
-  for (int v0 = 0; v0 < n && e == cudaSuccess;) {
-    long long lo = v0 + 1, hi = std::min<long long>(n, (long long)v0 + kRows);
-    while (lo < hi) {  // largest v1 <= hi whose rows fit the stage
-      const long long mid = (lo + hi + 1) / 2;
-      if (pre[(size_t)mid] - pre[(size_t)v0] <= stage_cap) lo = mid; else hi = mid - 1;
-    }
-    const int v1 = (int)lo;
-    for (int i = 0; i <= v1 - v0; ++i) prerel[(size_t)i] = pre[(size_t)v0 + i] - pre[(size_t)v0];
-    const long long cnt = pre[(size_t)v1] - pre[(size_t)v0];
-    e = cudaMemcpyAsync(dpre, prerel.data(), (size_t)(v1 - v0 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream);
-    if (e == cudaSuccess) e = launch_range_gather(gd, 0, v0, v1 - v0, dpre, dstage, ctx->stream);
-    if (e == cudaSuccess && cnt > 0)
-      e = cudaMemcpyAsync(rows.data(), dstage, (size_t)cnt * 4, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) break;
-    for (int v = v0; v < v1; ++v) {
-      const int L = live[(size_t)v];
-      const int* r = rows.data() + (pre[(size_t)v] - pre[(size_t)v0]);
-      ++gen;
-      for (int i = 0; i < L; ++i) {
-        const int u = r[i];
-        if (u < v) {
-          const int c = col[(size_t)u];
-          if (c <= L) stamp[(size_t)c] = gen;
-        }
-      }
-      int c = 0;
-      while (stamp[(size_t)c] == gen) ++c;
-      col[(size_t)v] = c;
-    }
-    v0 = v1;
+  cudaError_t e;
+  if (order == DC_ORDER_LDF)
+    e = cudaMemcpyAsync(prio, ctx->live, (size_t)n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+  else
+    e = cudaMemsetAsync(prio, 0, (size_t)n * 4, ctx->stream);
+  if (e == cudaSuccess) {
+    // fresh counters, queues and grid barrier for the launch
+    const size_t off = offsetof(DevState, bar_arrived);
+    e = cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + off, 0, sizeof(DevState) - off, ctx->stream);
   }
-  dfree(ctx, &dpre);
-  dfree(ctx, &dstage);
-  if (e != cudaSuccess) return cuda_fail(ctx, "greedy colouring", e);
-  if (n > 0) DC_CK(cudaMemcpyAsync(ctx->color, col.data(), (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
-  DC_CK(launch_color_max(graph_dev(ctx), ctx->st, ctx->stream));
-  DC_CK(cudaStreamSynchronize(ctx->stream));
+  if (e == cudaSuccess) e = cudaMemsetAsync(&ctx->st->cmax, 0, sizeof(int), ctx->stream);
+  if (e == cudaSuccess) {
+    RecolorParams rp = recolor_params(ctx, nullptr, 0);
+    rp.g.prop = prio;
+    rp.cp = cp;
+    rp.pred = pred;
+    rp.hri.min_live = 0;
+    rp.iter_cap = n + 1;  // every round colours at least one vertex
+    e = launch_init_color(rp, ctx->grid_recolor, ctx->stream);
+  }
+  if (e != cudaSuccess) {
+    drop();
+    return cuda_fail(ctx, "initial colouring launch", e);
+  }
+  s = read_state(ctx);
+  drop();
+  if (s != DC_OK) return s;
+  const unsigned st = ctx->h_st->status;
+  if (st & ST_TIMEOUT) {
+    ctx->broken = true;
+    return fail(ctx, DC_E_TIMEOUT, "a device-side grid barrier timed out");
+  }
+  if (st & (ST_OVERFLOW | ST_ITER)) return fail(ctx, DC_E_INTERNAL, "initial colouring: a capacity guard fired");
   return DC_OK;
 }
+
+dc_status dc_colors_init_greedy(dc_ctx* ctx) { return dc_colors_init(ctx, DC_ORDER_ID); }
 
 dc_status dc_apply_batch(dc_ctx* ctx, const dc_change* changes, int64_t k, dc_stats* out) {
   if (dc_status g_ = gate(ctx)) return g_;

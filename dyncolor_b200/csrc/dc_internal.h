@@ -192,6 +192,7 @@ struct RecolorParams {
   unsigned long long* cp;  // HB: n packed (degree property, colour) words
   HriBufs hri;             // HI: heavy-row index (hri.min_live == 0: off)
   unsigned char* lflag;  // k
+  int* pred;             // initial colouring: neighbours still to be coloured before each vertex
   // Batched mode: the graph is a disjoint union of independent graphs.
   const int* gid;        // vertex -> graph (nullptr: one graph)
   int ngraphs;
@@ -207,6 +208,11 @@ struct RecolorParams {
 // CUDA error of the launch.
 cudaError_t launch_struct(const StructParams& p, int grid, cudaStream_t s);
 cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s);
+// Initial colouring (greedy lowest free colour in a priority order) as a
+// Jones-Plassmann launch: p.g.prop holds each vertex's priority value (ties
+// and the id order: lower id first), p.cp and p.pred are n-sized scratch, the
+// colours land in p.g.color.
+cudaError_t launch_init_color(const RecolorParams& p, int grid, cudaStream_t s);
 int struct_kernel_occupancy();
 int recolor_kernel_occupancy();
 cudaError_t launch_validate(const GraphDev& g, unsigned long long* out, cudaStream_t s);

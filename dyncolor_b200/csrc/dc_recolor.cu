@@ -1236,6 +1236,256 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   }
 }
 
+// ---------------------------------------------------------------------
+// Initial colouring: greedy lowest free colour in a priority order, as a
+// Jones-Plassmann schedule (no reference counterpart: the reference takes
+// its initial colours from an external tool, MG/README.txt:19-22).
+//
+// A vertex is coloured once every neighbour before it in the order is
+// coloured, with the smallest colour none of those neighbours has.  Its
+// neighbours after it are then exactly the uncoloured ones, so every vertex
+// gets the colour the sequential greedy pass in that order gives it; the
+// rounds only run the independent vertices of the order side by side.
+// Order: larger g.prop first, ties by lower id (isPrior_RelativeOrdering's
+// comparison); with g.prop all zero it is the vertex-id order.
+//   P   pred[v] = neighbours before v         (all vertices, in units)
+//   F   frontier F0 = vertices with pred 0
+//   round (until the frontier is empty):
+//     R  mex over the neighbours before v      -> ncolor
+//     D  commit the colour; every neighbour after v loses one pred, and the
+//        ones that reach 0 form the next frontier
+// ---------------------------------------------------------------------
+namespace {
+
+// P over one unit (or a class-A batch of 32 rows): counts the neighbours of
+// each row that come before it.
+__device__ void pred_unit(Env& E, int4 un, int* pred) {
+  const GraphDev& g = E.g;
+  const int v = un.x;
+  const int L = g.len[v];
+  const long long o = g.off[v];
+  const int s_lo = un.y * E.CH, s_hi = min(L, s_lo + E.CH);
+  const int pv = g.prop[v];
+  int cnt = 0;
+  for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
+    const int sidx = s0 + lane_id();
+    const int u = sidx < s_hi ? g.adj[o + sidx] : -1;
+    if (u >= 0 && is_prior(g.prop[u], u, pv, v)) ++cnt;
+  }
+  cnt = (int)warp_sum_ll(cnt);
+  if (lane_id() == 0 && cnt) atomicAdd(&pred[v], cnt);
+}
+
+__device__ void pred_batchA(Env& E, const QueueBufs& qb, long long cA, long long b, int* pred) {
+  const GraphDev& g = E.g;
+  const long long idx = b * 32 + lane_id();
+  if (idx >= cA) return;
+  const int v = qb.itemsA[idx];
+  const int L = g.len[v];
+  const long long o = g.off[v];
+  const int pv = g.prop[v];
+  int cnt = 0;
+  for (int s = 0; s < L; ++s) {
+    const int u = g.adj[o + s];
+    if (u >= 0 && is_prior(g.prop[u], u, pv, v)) ++cnt;
+  }
+  if (cnt) atomicAdd(&pred[v], cnt);
+}
+
+// Pushes u into the next frontier through the warp buffer (all lanes call).
+__device__ __forceinline__ void push_ready(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int u, bool want) {
+  const unsigned bal = __ballot_sync(0xffffffffu, want);
+  if (!bal) return;
+  if (want) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = u;
+  __syncwarp();
+  pb.cnt += __popc(bal);
+  if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
+}
+
+// Commits v's colour (its first unit) into the colour word and the packed
+// word.
+__device__ __forceinline__ int commit_init(Env& E, int v) {
+  const int c = ld_cg(&E.p.ncolor[v]);
+  E.g.color[v] = c;
+  reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)c;
+  return c;
+}
+
+// D over one unit: every neighbour after v loses one pred; those reaching 0
+// are ready.
+__device__ void release_unit(Env& E, PushBuf& pb, int4 un, int* pred, const QueueBufs& nq, QCount* nc,
+                             int& cmax) {
+  const GraphDev& g = E.g;
+  const int v = un.x;
+  if (un.y == 0 && lane_id() == 0) cmax = max(cmax, commit_init(E, v));
+  const int L = g.len[v];
+  const long long o = g.off[v];
+  const int s_lo = un.y * E.CH, s_hi = min(L, s_lo + E.CH);
+  const int pv = g.prop[v];
+  for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
+    const int sidx = s0 + lane_id();
+    const int u = sidx < s_hi ? g.adj[o + sidx] : -1;
+    bool ready = false;
+    if (u >= 0 && is_prior(pv, v, g.prop[u], u)) ready = atomicSub(&pred[u], 1) == 1;
+    push_ready(E, pb, nq, nc, u, ready);
+  }
+}
+
+__device__ void release_batchA(Env& E, PushBuf& pb, const QueueBufs& qb, long long cA, long long b, int* pred,
+                               const QueueBufs& nq, QCount* nc, int& cmax) {
+  const GraphDev& g = E.g;
+  const long long idx = b * 32 + lane_id();
+  const bool valid = idx < cA;
+  const int v = valid ? qb.itemsA[idx] : 0;
+  if (valid) cmax = max(cmax, commit_init(E, v));
+  const int L = valid ? g.len[v] : 0;
+  const long long o = valid ? g.off[v] : 0;
+  const int pv = valid ? g.prop[v] : 0;
+  const int Lmax = __reduce_max_sync(0xffffffffu, L);
+  for (int s = 0; s < Lmax; ++s) {
+    const int u = s < L ? g.adj[o + s] : -1;
+    bool ready = false;
+    if (u >= 0 && is_prior(pv, v, g.prop[u], u)) ready = atomicSub(&pred[u], 1) == 1;
+    push_ready(E, pb, nq, nc, u, ready);
+  }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p) {
+  __shared__ Shared sh;
+  Env E;
+  E.p.bmA = p.bmA;
+  E.p.bmB = p.bmB;
+  E.p.bmC = p.bmC;
+  E.p.ncolor = p.ncolor;
+  E.g = p.g;
+  E.st = p.st;
+  E.variant = DC_HB;  // the prior-filtered mex of HB
+  E.CH = p.unit_slots;
+  E.my_scanned = 0;
+  E.gid = nullptr;
+  E.gpush = nullptr;
+  E.gchg = nullptr;
+  E.gskip = nullptr;
+  E.gf0 = nullptr;
+  E.cp = p.cp;
+  E.hri = p.hri;
+  E.hri_on = false;
+  E.hri_mex = false;
+  E.hri_split = false;
+  E.read_delta = 0;
+  DevState* st = p.st;
+  const GraphDev& g = E.g;
+  int* pred = p.pred;
+  unsigned bar = 0;
+  int ps = 0;
+  const long long gthreads = (long long)gridDim.x * blockDim.x;
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gwarp = gtid >> 5, nwarps = gthreads >> 5;
+  const bool leader = blockIdx.x == 0 && threadIdx.x == 0;
+  auto ctr = [&]() -> unsigned long long* {
+    if (leader) st->wctr[(ps + 1) % 3] = 0ull;
+    return &st->wctr[ps % 3];
+  };
+  if (leader) st->t_recolor[0] = globaltimer_ns();
+  // every vertex into the all-rows queue; packed (priority, colour) words
+  for (long long i0 = gwarp * 32; i0 < g.n; i0 += nwarps * 32) {
+    const long long v = i0 + lane_id();
+    if (v < g.n) {
+      pred[v] = 0;
+      E.cp[v] = ((unsigned long long)(unsigned)g.prop[v] << 32);
+    }
+    warp_push(p.qb[2], &st->q[Q_S1], g.len, v < g.n ? (int)v : -1, true, M_MEX_ALL, E.CH, &st->status);
+  }
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
+  // P
+  {
+    const QueueBufs& qb = p.qb[2];
+    const QCount* qc = &st->q[Q_S1];
+    const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
+    const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
+    const long long total = cU + (cA + 31) / 32;
+    unsigned long long* c = ctr();
+    while (true) {
+      const long long i = grab(c);
+      if (i >= total) break;
+      if (i < cU)
+        pred_unit(E, qb.units[i], pred);
+      else
+        pred_batchA(E, qb, cA, i - cU, pred);
+    }
+    ++ps;
+  }
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
+  // F0
+  for (long long i0 = gwarp * 32; i0 < g.n; i0 += nwarps * 32) {
+    const long long v = i0 + lane_id();
+    const bool r = v < g.n && ld_cg(&pred[v]) == 0;
+    warp_push(p.qb[0], &st->q[Q_LOOP0], g.len, r ? (int)v : -1, true, M_MEX_ALL, E.CH, &st->status);
+  }
+  if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
+  int fs = Q_LOOP0, fb = 0;
+  long long it = 0;
+  int cmax = -1;
+  while (ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU) > 0) {
+    if (it >= p.iter_cap) {
+      if (leader) atomicOr(&st->status, ST_ITER);
+      break;
+    }
+    ++it;
+    const int ns = (fs + 1) % 3;
+    const int nb = fb ^ 1;
+    if (leader) {
+      QCount* z = &st->q[(fs + 2) % 3];
+      z->countA = 0;
+      z->countU = 0;
+      z->masks = 0;
+    }
+    // R: the mex over the neighbours before each frontier vertex
+    phase_reduce(E, sh, p.qb[fb], &st->q[fs], ctr(), M_MEX_PRIOR, p.ncolor);
+    ++ps;
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
+    // D
+    {
+      const QueueBufs& fq = p.qb[fb];
+      const QCount* fc = &st->q[fs];
+      const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
+      const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
+      const long long total = cU + (cA + 31) / 32;
+      PushBuf pb;
+      pb.buf = sh.pbuf[warp_id()];
+      pb.cnt = 0;
+      unsigned long long* c = ctr();
+      while (true) {
+        const long long i = grab(c);
+        if (i >= total) break;
+        if (i < cU)
+          release_unit(E, pb, fq.units[i], pred, p.qb[nb], &st->q[ns], cmax);
+        else
+          release_batchA(E, pb, fq, cA, i - cU, pred, p.qb[nb], &st->q[ns], cmax);
+      }
+      if (pb.cnt > 0) flush(E, pb, p.qb[nb], &st->q[ns], pb.cnt);
+      ++ps;
+    }
+    if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
+    fs = ns;
+    fb = nb;
+  }
+  const int m = __reduce_max_sync(0xffffffffu, cmax);
+  if (lane_id() == 0 && m >= 0) atomicMax(&st->cmax, m);
+  if (leader) {
+    st->iterations = (unsigned long long)it;
+    st->t_recolor[1] = globaltimer_ns();
+  }
+}
+
+cudaError_t launch_init_color(const RecolorParams& p, int grid, cudaStream_t s) {
+  RecolorParams q = p;
+  void* args[] = {&q};
+  return cudaLaunchCooperativeKernel((const void*)init_color_kernel, dim3(grid), dim3(kThreads), args, 0, s);
+}
+
 cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s) {
   RecolorParams q = p;
   void* args[] = {&q};
@@ -1244,11 +1494,13 @@ cudaError_t launch_recolor(const RecolorParams& p, int grid, cudaStream_t s) {
 }
 
 int recolor_kernel_occupancy() {
-  int a = 0, b = 0;
+  int a = 0, b = 0, c = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, recolor_kernel<DC_HI>, kThreads, 0) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recolor_kernel<DC_HB>, kThreads, 0) != cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, recolor_kernel<DC_HB>, kThreads, 0) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, init_color_kernel, kThreads, 0) != cudaSuccess)
     return 0;
-  return a < b ? a : b;
+  const int ab = a < b ? a : b;
+  return ab < c ? ab : c;
 }
 
 }  // namespace dc

@@ -135,11 +135,23 @@ dc_status dc_graph_load_edges(dc_ctx* ctx, int32_t n, const int32_t* a, const in
 /* initial-color (read_Input_Color): colours must lie in [0, 2^30). */
 dc_status dc_colors_set(dc_ctx* ctx, const int32_t* colors, int32_t n);
 
+/* Orders of the initial colouring. */
+typedef enum {
+  DC_ORDER_ID = 0, /* vertex-id order */
+  DC_ORDER_LDF = 1 /* largest live degree first, ties by lower id */
+} dc_order;
+
 /* Initial colouring of the resident graph, not in the reference (whose
- * initial colours come from an external tool, MG/README.txt:19-22): greedy
- * lowest free colour in vertex-id order over the current edge set.  The
- * rows are read back to the host and coloured there, since the greedy order
- * is serial; the result equals dcg_greedy_color on the same edges. */
+ * initial colours come from an external tool, MG/README.txt:19-22): the
+ * greedy lowest-free colouring in the given order over the current edge set,
+ * computed on the device as a Jones-Plassmann schedule (a vertex is coloured
+ * as soon as every neighbour before it in the order is).  The colours equal
+ * the sequential greedy pass in that order: with DC_ORDER_ID they are
+ * dcg_greedy_color's on the same edges.  DC_ORDER_LDF re-seeds a colouring
+ * with the largest-degree-first order, which usually needs fewer colours. */
+dc_status dc_colors_init(dc_ctx* ctx, int32_t order);
+
+/* dc_colors_init(ctx, DC_ORDER_ID). */
 dc_status dc_colors_init_greedy(dc_ctx* ctx);
 
 /* apply-update-batch from host memory (any host pointer; pinned is fastest).

@@ -336,6 +336,41 @@ int orc_greedy_id_order(orc_graph* g) {
   return ORC_OK;
 }
 
+/* Greedy lowest-free colour with the vertices taken in the given order
+ * (order[i] = the i-th vertex coloured); the colour of a vertex is the mex
+ * over its neighbours coloured before it.  Checker for the device's
+ * initial colouring in any order. */
+int orc_greedy_in_order(orc_graph* g, const int32_t* order) {
+  scratch_t s = {0};
+  if (scratch_fit(&s, (int64_t)max_len(g) + 2)) return ORC_E_NOMEM;
+  uint8_t* done = (uint8_t*)calloc(g->n > 0 ? (size_t)g->n : 1, 1);
+  if (!done) {
+    free(s.stamp);
+    return ORC_E_NOMEM;
+  }
+  for (int32_t i = 0; i < g->n; ++i) {
+    int32_t v = order[i];
+    if (v < 0 || v >= g->n || done[v]) {
+      free(done);
+      free(s.stamp);
+      return ORC_E_INVAL;
+    }
+    uint32_t gen = scratch_next(&s);
+    int32_t L = g->len[v];
+    for (int32_t j = 0; j < L; ++j) {
+      int32_t u = g->row[v][j];
+      if (u >= 0 && done[u] && g->color[u] <= L) s.stamp[g->color[u]] = gen;
+    }
+    int32_t c = 0;
+    while (c <= L && s.stamp[c] == gen) ++c;
+    g->color[v] = c;
+    done[v] = 1;
+  }
+  free(done);
+  free(s.stamp);
+  return ORC_OK;
+}
+
 /* ------------------------------------------------------------------ */
 /* batch application                                                   */
 /* ------------------------------------------------------------------ */

@@ -97,6 +97,8 @@ int32_t orc_neighbors(const orc_graph* g, int32_t v, int32_t* out, int32_t cap);
 int orc_is_greedy_id_order(const orc_graph* g);
 /* Greedy lowest-free colour in vertex-id order (same rule as above). */
 int orc_greedy_id_order(orc_graph* g);
+/* Greedy lowest-free colour with vertices taken in order[0..n). */
+int orc_greedy_in_order(orc_graph* g, const int32_t* order);
 int32_t orc_num_vertices(const orc_graph* g);
 void orc_set_threads(int nthreads);
 void orc_set_instrument(int on);

@@ -71,6 +71,7 @@ def lib():
         L.orc_neighbors.argtypes = [P, C.c_int32, P, C.c_int32]
         L.orc_is_greedy_id_order.argtypes = [P]
         L.orc_greedy_id_order.argtypes = [P]
+        L.orc_greedy_in_order.argtypes = [P, P]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_set_instrument.argtypes = [C.c_int]
         # seeded workload generators (dc_gen.cpp compiled into this library)
@@ -161,6 +162,10 @@ class Graph:
 
     def is_greedy_id_order(self) -> bool:
         return lib().orc_is_greedy_id_order(self._g) == 1
+
+    def greedy_in_order(self, order) -> int:
+        o = np.ascontiguousarray(order, dtype=np.int32)
+        return lib().orc_greedy_in_order(self._g, _ptr(o))
 
     def greedy_id_order(self) -> int:
         return lib().orc_greedy_id_order(self._g)

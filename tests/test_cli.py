@@ -63,9 +63,13 @@ def test_cli_on_reference_fixture_and_golden_cases(golden, tmp_path):
         want_it, want_status = c["snapshot_iters"]
         if want_status != 0:
             continue  # capped runs are covered by the library tests
-        if r.returncode != 0:
+        # exit status 1 means the result has a monochromatic edge: the random
+        # golden cases start from arbitrary colourings, which the
+        # recolouring only repairs around the changed edges
+        if r.returncode not in (0, 1) or (c["name"].startswith("sample") and r.returncode != 0):
             bad.append((c["name"], r.returncode, r.stderr[-300:]))
             continue
+        assert (r.returncode == 1) == ("##Error found" in r.stdout)
         got = np.zeros(n, np.int32)
         for line in open(out):
             v, x = line.split()
