@@ -52,7 +52,8 @@ class Options(C.Structure):
         ("cuda_graph", C.c_int32),
         ("heavy_min_live", C.c_int32),
         ("barrier_timeout_ms", C.c_int32),
-        ("reserved", C.c_int32 * 4),
+        ("grid_ctas", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -177,7 +178,7 @@ class Context:
     def __init__(self, variant: int = HI, device: int = 0, iter_cap: int = 0, slack: float = 0.0,
                  blocks_per_sm: int = 0, unit_slots: int = 0, stream: int | None = None,
                  reserve_slots: int = 0, cuda_graph: bool = False, heavy_min_live: int = 0,
-                 barrier_timeout_ms: int = 0):
+                 barrier_timeout_ms: int = 0, grid_ctas: int = 0):
         L = lib()
         opt = Options()
         L.dc_options_default(C.byref(opt))
@@ -195,6 +196,7 @@ class Context:
         opt.heavy_min_live = int(heavy_min_live)
         if barrier_timeout_ms:
             opt.barrier_timeout_ms = int(barrier_timeout_ms)
+        opt.grid_ctas = int(grid_ctas)
         opt.stream = stream
         h = C.c_void_p()
         rc = L.dc_create(C.byref(h), C.byref(opt))

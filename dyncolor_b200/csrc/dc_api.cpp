@@ -50,12 +50,15 @@ int unit_slots(const dc_ctx* c) { return c->opt.unit_slots; }
 dc_status ensure_recolor_scratch(dc_ctx* ctx) {
   if (ctx->rc_pool_cap == ctx->pool_cap) return DC_OK;
   const long long n = std::max(ctx->n, 1);
-  const long long CH = unit_slots(ctx);
+  // the loop cuts units down to an eighth of unit_slots (at least 128) when
+  // a frontier is small
+  const long long CH = std::max<long long>(128, (unit_slots(ctx) / 8) & ~127ll);
   const long long capU = n + ctx->pool_cap / CH + 64;
-  // mask words: a multi-unit row (length L > CH) takes at most L/32 + 7
-  // words in the mex modes and 132 words for saturation sizes (buffer 2)
+  // mask words: a multi-unit row (length L > its unit size) takes at most
+  // L/32 + 7 words in the mex modes and 132 words for saturation sizes
+  // (buffer 2, cut at unit_slots)
   const long long capM_mex = ctx->pool_cap / 32 + 8 * (ctx->pool_cap / CH) + 1024;
-  const long long capM_dist = std::max(capM_mex, 132 * (ctx->pool_cap / CH) + 1024);
+  const long long capM_dist = std::max(capM_mex, 132 * (ctx->pool_cap / unit_slots(ctx)) + 1024);
   const long long words = (n + 31) / 32 + 1;
   dc_status s;
   for (int b = 0; b < 3; ++b) {
@@ -634,6 +637,10 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   }
   ctx->grid_struct = ctx->sms * occ_s;
   ctx->grid_recolor = ctx->sms * occ_r;
+  if (o.grid_ctas > 0) {
+    ctx->grid_struct = std::min(ctx->grid_struct, (int)o.grid_ctas);
+    ctx->grid_recolor = std::min(ctx->grid_recolor, (int)o.grid_ctas);
+  }
   if (o.stream) {
     ctx->stream = (cudaStream_t)o.stream;
   } else {

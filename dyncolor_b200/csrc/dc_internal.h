@@ -40,7 +40,7 @@ struct QCount {
   unsigned long long countA;  // class A items
   unsigned long long countU;  // work units (class B/C)
   unsigned long long masks;   // multi-unit mask words handed out
-  unsigned long long pad;
+  unsigned long long ch;      // slots per work unit of the queue's units (0: unit_slots)
 };
 
 // Lives in device memory.  Fields up to `pool_used_start` persist across
@@ -156,7 +156,7 @@ struct StructParams {
 // colour.
 constexpr int kHeavyMinLive = 2048;
 // A batch uses the index when lines * kIndexBatchRatio >= n.
-constexpr long long kIndexBatchRatio = 32;
+constexpr long long kIndexBatchRatio = 256;
 constexpr int kHriBins = 1024;  // exact colour order below 1023; colours >= 1023 share the first bin
 struct HriBufs {
   int* hid;                   // n: index of v's ordered copy, or -1
@@ -168,7 +168,8 @@ struct HriBufs {
   int* xv;                    // cap_exc: changed neighbours
   unsigned* bmF;              // n/32 + 1: colour changed since the index was built
   int2* alist;                // cap_a: (vertex, chunk) of first changes, for the append phase
-  int* hist;                  // cap_hist * kHriBins: row i's neighbour count per colour at build time
+  int* hist;                  // cap_hist * kHriBins: row i's count of neighbours per launch-start colour
+                              // that have not changed colour since (the append phase takes them off)
   int* hsplit;                // HB, cap_rows: row i's copy holds its prior neighbours first, hsplit[i]
                               // of them, then the rest
   long long cap_rows, cap_pairs, cap_exc, cap_a, cap_hist;

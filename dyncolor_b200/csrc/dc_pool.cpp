@@ -492,6 +492,7 @@ dc_status dc_pool_create(dc_pool** out, const dc_pool_options* opt) {
   co.iter_cap = o.iter_cap;
   co.slack = o.slack;
   co.blocks_per_sm = o.blocks_per_sm;
+  co.grid_ctas = o.grid_ctas;
   co.unit_slots = o.unit_slots;
   co.cuda_graph = o.cuda_graph;
   dc_pool* P = new (std::nothrow) dc_pool();

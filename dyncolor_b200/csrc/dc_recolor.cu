@@ -107,6 +107,20 @@ __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const
   }
 }
 
+// Slots per work unit for a queue pushed while processing a phase of
+// `items` work items with `nwarps` warps: the configured size while the
+// phase keeps every warp busy, a quarter or an eighth of it (at least 128,
+// a multiple of 128) when it does not.
+__device__ __forceinline__ int unit_slots_for(long long items, long long nwarps, int ch) {
+  int d = 1;
+  if (items < nwarps / 2)
+    d = 8;
+  else if (items < 2 * nwarps)
+    d = 4;
+  const int c = (ch / d) & ~127;
+  return c < 128 ? 128 : c;
+}
+
 // Largest j (0..31) with excl_j <= s, excl held one value per lane and
 // non-decreasing across lanes.  All lanes must call.
 __device__ __forceinline__ int find_owner(int excl, int s) {
@@ -145,7 +159,8 @@ struct Env {
   GraphDev g;
   DevState* st;
   int variant;
-  int CH;
+  int CH;   // slots per work unit of the queue being processed
+  int CHp;  // slots per work unit of the units this phase pushes
   long long my_scanned;
   // HB: (degree property << 32) | colour word per vertex, so one 8-byte
   // gather gives both; the next-frontier mark lives in its colour half
@@ -237,12 +252,15 @@ __device__ __forceinline__ void fold_low(unsigned* sm, unsigned long long lm) {
 
 // HI mex of an indexed row v inside the loop, from the index instead of a
 // gather per neighbour: colour c is present iff some neighbour that kept
-// its launch-start colour has colour c (the row's colour-c segment of the
-// ordered copy holds a vertex not marked as changed), or some changed
-// neighbour has colour c now (its change list).  Colours are tried in
-// increasing order 32 at a time.  Returns false when the row has no usable
-// index (the caller scans it); the whole row is handled by its first unit.
-__device__ bool reduce_heavy(Env& E, Shared& sh, int4 un, int* out) {
+// its launch-start colour has colour c (the row's count of unchanged
+// neighbours of launch-start colour c is above 0: the build counted every
+// colour and the append phase takes one off for each neighbour's first
+// change), or some changed neighbour has colour c now (its change list).
+// Every unit of the row gathers the current colours of its slice of the
+// change list into the row's mask; the unit that finishes last reads the
+// counts 32 colours at a time from 0.  Returns false when the row has no
+// usable index (the caller scans it).
+__device__ bool reduce_heavy(Env& E, Shared& sh, const QueueBufs& qb, int4 un, int* out) {
   const HriBufs& H = E.hri;
   const int v = un.x;
   const int hi = H.hid[v];
@@ -250,50 +268,65 @@ __device__ bool reduce_heavy(Env& E, Shared& sh, int4 un, int* out) {
   const long long xb = H.xoff[hi];
   const int xc = ld_cg(&H.xcnt[hi]);
   if ((long long)xc > H.xoff[hi + 1] - xb) return false;  // change list overflowed
-  if (un.y != 0) return true;
-  const long long pe = H.hoff[hi + 1];
-  if (lane_id() == 0) E.my_scanned += pe - H.hoff[hi];  // the rule covers every live entry
+  const int nch = un.w;
+  const int nw = mask_words(E.g.len[v], M_MEX_ALL);  // as the queue push sized the row's mask
   unsigned* sm = sh.mask[warp_id()];
-  for (int k = lane_id(); k < kMaskWords; k += 32) sm[k] = 0;
+  for (int k = lane_id(); k < nw; k += 32) sm[k] = 0;
   __syncwarp();
-  for (int j = lane_id(); j < xc; j += 32) {
-    const int u = H.xv[xb + j];
-    const int c = E.g.color[u] & kColorMask;
-    if (c < kMaskBits) atomicOr(&sm[c >> 5], 1u << (c & 31));
+  const long long e0 = (long long)un.y * E.CH;
+  const long long e1 = min((long long)xc, e0 + E.CH);
+  for (long long r0 = e0; r0 < e1; r0 += 128) {
+    int cc[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const long long idx = r0 + j * 32 + lane_id();
+      cc[j] = idx < e1 ? (E.g.color[H.xv[xb + idx]] & kColorMask) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (cc[j] >= 0 && cc[j] < nw * 32) atomicOr(&sm[cc[j] >> 5], 1u << (cc[j] & 31));
   }
   __syncwarp();
-  const int* hist = H.hist + (long long)hi * kHriBins;
-  long long below = 0;  // neighbours (at launch start) with a colour below the chunk
-  long long reads = xc;
+  if (lane_id() == 0 && e1 > e0) E.read_delta += e1 - e0;
+  if (nch > 1) {
+    unsigned* gm = qb.gmask + un.z;  // [0]: finished units, [1..nw]: mask
+    for (int k = lane_id(); k < nw; k += 32) {
+      const unsigned x = sm[k];
+      if (x) atomicOr(&gm[1 + k], x);
+    }
+    __threadfence();
+    __syncwarp();
+    int last = 0;
+    if (lane_id() == 0) last = atomicAdd(&gm[0], 1u) == (unsigned)(nch - 1);
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return true;
+    __threadfence();
+    for (int k = lane_id(); k < nw; k += 32) sm[k] = ld_cg(&gm[1 + k]);
+    __syncwarp();
+  }
+  const long long live = H.hoff[hi + 1] - H.hoff[hi];
+  const int* cnt = H.hist + (long long)hi * kHriBins;
   int r = -1;
   for (int c0 = 0; c0 < kHriBins - 1; c0 += 32) {
     const int c = c0 + lane_id();
-    const int cnt = c < kHriBins - 1 ? hist[c] : 0;
-    const int incl = warp_incl_scan(cnt);
-    // colour c's segment: the copy is descending, so it ends where the
-    // colours below c begin
-    const long long seg_end = pe - (below + incl - cnt);
-    bool pres = c >= kHriBins - 1 || ((sm[c >> 5] >> (c & 31)) & 1u);
-    for (int q = 1; !pres && q <= cnt; ++q) {
-      const int u = (int)(unsigned)H.pairs[seg_end - q];
-      ++reads;
-      pres = !((ld_cg(&H.bmF[u >> 5]) >> (u & 31)) & 1u);
-    }
+    bool pres = true;
+    if (c < kHriBins - 1) pres = ld_cg(&cnt[c]) > 0 || (c < nw * 32 && ((sm[c >> 5] >> (c & 31)) & 1u));
     const unsigned bal = __ballot_sync(0xffffffffu, pres);
-    below += __shfl_sync(0xffffffffu, incl, 31);
     if (bal != 0xffffffffu) {
       r = c0 + __ffs(~bal) - 1;
       break;
     }
   }
+  long long extra = 0;
   if (r < 0) {
     // every colour below the shared top bin is present: scan the row
-    reads += pe - H.hoff[hi];
+    extra = E.g.len[v];
     r = slow_mex(E, sm, v, M_MEX_ALL, 0);
   }
   if (lane_id() == 0) {
     out[v] = r;
-    E.read_delta += reads - (pe - H.hoff[hi]);
+    E.my_scanned += live;  // the rule covers every live entry
+    E.read_delta += extra - live;
   }
   __syncwarp();
   return true;
@@ -347,7 +380,7 @@ __device__ bool reduce_split(Env& E, Shared& sh, int4 un, int* out) {
 }
 
 __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, int mode, int* out) {
-  if (E.hri_mex && mode == M_MEX_ALL && reduce_heavy(E, sh, un, out)) return;
+  if (E.hri_mex && mode == M_MEX_ALL && reduce_heavy(E, sh, qb, un, out)) return;
   if (E.hri_split && mode == M_MEX_PRIOR && reduce_split(E, sh, un, out)) return;
   const GraphDev& g = E.g;
   const int v = un.x, chunk = un.y, ms = un.z, nch = un.w;
@@ -548,7 +581,7 @@ __device__ __forceinline__ void flush(Env& E, PushBuf& pb, const QueueBufs& nq, 
   const int u = lane_id() < k ? pb.buf[lane_id()] : -1;
   __syncwarp();
   if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
-  warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CH, &E.st->status);
+  warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CHp, &E.st->status);
   // keep the remainder at the front
   const int rest = pb.cnt - k;
   if (lane_id() < rest) pb.buf[lane_id()] = pb.buf[k + lane_id()];  // rest <= 31 < k
@@ -655,12 +688,14 @@ __device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi
   if (lane_id() == 0) E.read_delta += reads - (p1 > p0 ? p1 - p0 : 0);
 }
 
-// First colour change of v since the index was built: queue v's row, in
-// chunks, for the append phase.  An overflowing queue turns the index off
-// for the rest of the batch.
+// First colour change of v since the index was built (c0: its colour
+// until then): queue v's row, in chunks, for the append phase.  An item is
+// (v, chunk | bin << 21), bin = c0's count bin.  An overflowing queue turns
+// the index off for the rest of the batch.
 constexpr int kAppendChunk = 512;  // slots per append-phase item: 4 rounds of 4 loads per lane
+constexpr int kChunkBits = 21;     // rows of up to 2^21 append chunks (2^30 slots)
 
-__device__ __forceinline__ void push_first(Env& E, int v) {
+__device__ __forceinline__ void push_first(Env& E, int v, int c0) {
   const int L = E.g.len[v];
   const int c = L > 0 ? (L + kAppendChunk - 1) / kAppendChunk : 0;
   if (c == 0) return;
@@ -669,11 +704,14 @@ __device__ __forceinline__ void push_first(Env& E, int v) {
     atomicExch(&E.st->hri_off, 1u);
     return;
   }
-  for (int q = 0; q < c; ++q) E.hri.alist[b + q] = make_int2(v, q);
+  const int bin = c0 < kHriBins - 1 ? c0 : kHriBins - 1;
+  for (int q = 0; q < c; ++q) E.hri.alist[b + q] = make_int2(v, q | (bin << kChunkBits));
 }
 
 // Append phase: every vertex whose colour changed for the first time since
-// the index was built joins the change list of each indexed neighbour.
+// the index was built joins the change list of each indexed neighbour, and
+// leaves that neighbour's count of unchanged neighbours of its launch-start
+// colour.
 __device__ void phase_append(Env& E, unsigned long long* ctr) {
   const HriBufs& H = E.hri;
   // an overflowed queue has unwritten items, and the index is off anyway
@@ -684,9 +722,11 @@ __device__ void phase_append(Env& E, unsigned long long* ctr) {
     if (i >= cnt) break;
     const int2 it = H.alist[i];
     const int v = it.x;
+    const int chunk = it.y & ((1 << kChunkBits) - 1);
+    const int bin = it.y >> kChunkBits;
     const int L = E.g.len[v];
     const long long o = E.g.off[v];
-    const int s_lo = it.y * kAppendChunk, s_hi = min(L, s_lo + kAppendChunk);
+    const int s_lo = chunk * kAppendChunk, s_hi = min(L, s_lo + kAppendChunk);
     for (int r0 = s_lo; r0 < s_hi; r0 += 128) {
       int uu[4], hh[4];
 #pragma unroll
@@ -702,6 +742,7 @@ __device__ void phase_append(Env& E, unsigned long long* ctr) {
         const int h = hh[j];
         const int slot = atomicAdd(&H.xcnt[h], 1);
         if ((long long)slot < H.xoff[h + 1] - H.xoff[h]) H.xv[H.xoff[h] + slot] = v;
+        if (h < H.cap_hist && bin < kHriBins - 1) atomicSub(&H.hist[(long long)h * kHriBins + bin], 1);
       }
     }
   }
@@ -875,6 +916,145 @@ __device__ __forceinline__ int queue_item(const QueueBufs& qb, long long cA, lon
   return -1;
 }
 
+// Pushes u into the next frontier through the warp buffer (all lanes call).
+__device__ __forceinline__ void push_ready(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int u, bool want) {
+  const unsigned bal = __ballot_sync(0xffffffffu, want);
+  if (!bal) return;
+  if (want) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = u;
+  __syncwarp();
+  pb.cnt += __popc(bal);
+  if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
+}
+
+// HB findEligibleNeighbors for a dense frontier, by pulling: rather than
+// every frontier vertex walking its whole row (every entry covered by the
+// rule), every vertex u asks whether it is marked, and stops at the first
+// reason.  u is marked iff a neighbour prior to u is in the frontier, or u
+// is in the frontier and a neighbour prior to u has u's colour -- the same
+// set the rule marks from the frontier side (HB/gpuFunctions_undir.cuh:
+// 259-291).  Frontier membership is a bitmap built from the queue first.
+constexpr int kPullLane = 64;  // rows up to this length are walked by one lane
+
+// Sets the membership bit of every frontier vertex and counts the entries
+// the rule covers (the frontier rows' live entries).
+__device__ void phase_mark_frontier(Env& E, const QueueBufs& fq, const QCount* fc, unsigned* inF,
+                                    long long gwarp, long long nwarps) {
+  const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
+  const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
+  const long long total = cA + cU;
+  long long cov = 0;
+  for (long long i0 = gwarp * 32; i0 < total; i0 += nwarps * 32) {
+    const int v = queue_item(fq, cA, total, i0 + lane_id());
+    if (v < 0) continue;
+    if (E.gskip && ld_cg(&E.gskip[E.gid[v]]) == 0) continue;  // its graph has stopped
+    atomicOr(&inF[v >> 5], 1u << (v & 31));
+    cov += E.g.live[v];
+  }
+  cov = warp_sum_ll(cov);
+  if (lane_id() == 0) {
+    E.my_scanned += cov;
+    E.read_delta -= cov;
+  }
+}
+
+__device__ __forceinline__ bool in_bits(const unsigned* bm, int v) { return (ld_cg(&bm[v >> 5]) >> (v & 31)) & 1u; }
+
+// Walks u's neighbours prior to u (an indexed row lists them first) until
+// one is in the frontier, or -- when u is in the frontier -- has u's colour.
+// One lane.
+__device__ __forceinline__ bool pull_lane(const Env& E, const unsigned* inF, int u, long long& reads) {
+  const GraphDev& g = E.g;
+  const int L = g.len[u];
+  const long long o = g.off[u];
+  const int pu = g.prop[u];
+  const bool fu = in_bits(inF, u);
+  const int cu = (int)((unsigned)E.cp[u] & (unsigned)kColorMask);
+  for (int s = 0; s < L; ++s) {
+    const int w = g.adj[o + s];
+    if (w < 0) continue;
+    ++reads;
+    const unsigned long long x = E.cp[w];
+    if (!is_prior((int)(x >> 32), w, pu, u)) continue;
+    if (in_bits(inF, w) || (fu && (int)((unsigned)x & (unsigned)kColorMask) == cu)) return true;
+  }
+  return false;
+}
+
+// The same for a long row, by the whole warp (all lanes call; u uniform).
+__device__ bool pull_warp(const Env& E, const unsigned* inF, int u, long long& reads) {
+  const GraphDev& g = E.g;
+  const int pu = g.prop[u];
+  const bool fu = in_bits(inF, u);
+  const int cu = (int)((unsigned)E.cp[u] & (unsigned)kColorMask);
+  const int hi = E.hri_split ? E.hri.hid[u] : -1;
+  if (hi >= 0) {
+    // prior neighbours first: only they can mark u
+    const long long pb = E.hri.hoff[hi];
+    const int nh = E.hri.hsplit[hi];
+    for (int s0 = 0; s0 < nh; s0 += 32) {
+      const int s = s0 + lane_id();
+      bool hit = false;
+      if (s < nh) {
+        const int w = (int)(unsigned)E.hri.pairs[pb + s];
+        hit = in_bits(inF, w) ||
+              (fu && (int)((unsigned)E.cp[w] & (unsigned)kColorMask) == cu);
+      }
+      reads += min(32, nh - s0);
+      if (__any_sync(0xffffffffu, hit)) return true;
+    }
+    return false;
+  }
+  const int L = g.len[u];
+  const long long o = g.off[u];
+  for (int s0 = 0; s0 < L; s0 += 32) {
+    const int s = s0 + lane_id();
+    bool hit = false;
+    const int w = s < L ? g.adj[o + s] : -1;
+    if (w >= 0) {
+      const unsigned long long x = E.cp[w];
+      hit = is_prior((int)(x >> 32), w, pu, u) &&
+            (in_bits(inF, w) || (fu && (int)((unsigned)x & (unsigned)kColorMask) == cu));
+    }
+    reads += min(32, L - s0);
+    if (__any_sync(0xffffffffu, hit)) return true;
+  }
+  return false;
+}
+
+// Every vertex decides whether it joins the next frontier; lanes take rows
+// of up to kPullLane slots, the warp then takes the longer rows of its 32
+// vertices one by one.
+__device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const QueueBufs& nq, QCount* nc,
+                              long long gwarp, long long nwarps) {
+  const GraphDev& g = E.g;
+  PushBuf pb;
+  pb.buf = sh.pbuf[warp_id()];
+  pb.cnt = 0;
+  long long reads = 0;
+  for (long long b0 = gwarp * 32; b0 < g.n; b0 += nwarps * 32) {
+    const long long ul = b0 + lane_id();
+    int u = ul < g.n ? (int)ul : -1;
+    if (u >= 0 && E.gskip && ld_cg(&E.gskip[E.gid[u]]) == 0) u = -1;  // its graph has stopped
+    const bool lng = u >= 0 && (g.len[u] > kPullLane || (E.hri_split && E.hri.hid[u] >= 0));
+    bool want = false;
+    if (u >= 0 && !lng) want = pull_lane(E, inF, u, reads);
+    push_ready(E, pb, nq, nc, u, want);
+    unsigned todo = __ballot_sync(0xffffffffu, lng);
+    while (todo) {
+      const int l = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int x = __shfl_sync(0xffffffffu, u, l);
+      long long r = 0;
+      const bool m = pull_warp(E, inF, x, r);
+      if (lane_id() == 0) reads += r;
+      push_ready(E, pb, nq, nc, x, m && lane_id() == 0);
+    }
+  }
+  if (pb.cnt > 0) flush(E, pb, nq, nc, pb.cnt);
+  reads = warp_sum_ll(reads);
+  if (lane_id() == 0) E.read_delta += reads;
+}
+
 __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int kind,
                              const QueueBufs* f0, QCount* f0c, long long gwarp, long long nwarps,
                              unsigned long long* items_stat, int* chg_flag) {
@@ -889,6 +1069,7 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
     const int v = queue_item(qb, cA, total, i0 + lane_id());
     int push = -1;
     int first = -1;  // first colour change since the heavy-row index was built
+    int first_c0 = 0;  // its colour until then
     if (v >= 0) {
       ++items;
       switch (kind) {
@@ -899,7 +1080,10 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           if (nc != oc) {
             changed = true;
             if (E.gchg) atomicAdd(&E.gchg[E.gid[v]], 1);
-            if (E.hri_on && mark_bit(E.hri.bmF, v)) first = v;
+            if (E.hri_on && mark_bit(E.hri.bmF, v)) {
+              first = v;
+              first_c0 = oc;
+            }
           }
           g.color[v] = nc;  // also clears the frontier mark
           if (E.cp) reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)nc;
@@ -911,7 +1095,10 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           const int nc = ld_cg(&E.p.ncolor[v]);
           const int oc = g.color[v];
           if (nc != oc) {
-            if (E.hri_on && mark_bit(E.hri.bmF, v)) first = v;
+            if (E.hri_on && mark_bit(E.hri.bmF, v)) {
+              first = v;
+              first_c0 = oc;
+            }
             if (kind == C_SEED_DEL) g.prev[v] = oc;
             g.color[v] = nc;
             if (E.cp) reinterpret_cast<unsigned*>(E.cp + v)[0] = (unsigned)nc;
@@ -923,7 +1110,10 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
         }
         case C_SEED_INS: {
           const int nc = ld_cg(&E.p.ncolor[v]);
-          if (E.hri_on && nc != g.color[v] && mark_bit(E.hri.bmF, v)) first = v;
+          if (E.hri_on && nc != g.color[v] && mark_bit(E.hri.bmF, v)) {
+            first = v;
+            first_c0 = g.color[v];
+          }
           g.prev[v] = g.color[v];
           g.color[v] = nc;
           cmax_local = max(cmax_local, nc);
@@ -939,11 +1129,11 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
           break;
       }
     }
-    if (first >= 0) push_first(E, first);
+    if (first >= 0) push_first(E, first, first_c0);
     if (f0) {
       const bool claim = push >= 0 && mark_bit(E.p.bmB, push);
       if (claim && E.gf0) atomicAdd(&E.gf0[E.gid[push]], 1);
-      warp_push(*f0, f0c, g.len, claim ? push : -1, true, M_MEX_ALL, E.CH, &E.st->status);
+      warp_push(*f0, f0c, g.len, claim ? push : -1, true, M_MEX_ALL, E.CHp, &E.st->status);
     }
   }
   const int m = __reduce_max_sync(0xffffffffu, cmax_local);
@@ -969,6 +1159,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.st = p.st;
   E.variant = V;
   E.CH = p.unit_slots;
+  E.CHp = p.unit_slots;
   E.my_scanned = 0;
   E.gid = p.gid;
   E.gpush = nullptr;
@@ -1177,8 +1368,27 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
           E.gskip = nullptr;
         }
       }
-      phase_expand(E, sh, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
-      ++ps;
+      // Work units: the frontier's units were cut at the size recorded with
+      // its queue; the next frontier's are cut smaller when this one is
+      // small, so a small phase is not set by a few long units.
+      {
+        const unsigned long long fch = ld_cg(&st->q[fs].ch);
+        E.CH = fch ? (int)fch : p.unit_slots;
+        const long long items = (long long)ld_cg(&st->q[fs].countU) + ((long long)ld_cg(&st->q[fs].countA) + 31) / 32;
+        E.CHp = unit_slots_for(items, nwarps, p.unit_slots);
+        if (leader) st->q[ns].ch = (unsigned long long)E.CHp;
+      }
+      // HB with a frontier of more than a sixteenth of the vertices pulls
+      const bool pull = V == DC_HB &&
+                        (long long)(ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU)) * 16 > (long long)g.n;
+      if (pull) {
+        phase_mark_frontier(E, p.qb[fb], &st->q[fs], p.bmC, gwarp, nwarps);
+        if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
+        phase_pull_hb(E, sh, p.bmC, p.qb[nb], &st->q[ns], gwarp, nwarps);
+      } else {
+        phase_expand(E, sh, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
+        ++ps;
+      }
       if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       lap(1);
       const QCount* nc = &st->q[ns];
@@ -1199,6 +1409,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         }
         E.gchg = V == DC_HB ? cur : nullptr;
       }
+      E.CH = E.CHp;  // the units E just pushed
       phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
       ++ps;
       if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
@@ -1206,6 +1417,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       // C
       phase_commit(E, p.qb[nb], nc, C_LOOP, nullptr, nullptr, gwarp, nwarps, &st->frontier_total,
                    &st->chg[it & 1]);
+      if (pull) {
+        // clear the frontier membership bits for the next pulling iteration
+        const long long words = ((long long)g.n + 31) / 32 + 1;
+        for (long long w = gtid; w < words; w += gthreads) p.bmC[w] = 0u;
+      }
       if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       if (E.hri_on && ld_cg(&st->a_count) > 0) {
         phase_append(E, ctr());
@@ -1292,16 +1508,6 @@ __device__ void pred_batchA(Env& E, const QueueBufs& qb, long long cA, long long
   if (cnt) atomicAdd(&pred[v], cnt);
 }
 
-// Pushes u into the next frontier through the warp buffer (all lanes call).
-__device__ __forceinline__ void push_ready(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int u, bool want) {
-  const unsigned bal = __ballot_sync(0xffffffffu, want);
-  if (!bal) return;
-  if (want) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = u;
-  __syncwarp();
-  pb.cnt += __popc(bal);
-  if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
-}
-
 // Commits v's colour (its first unit) into the colour word and the packed
 // word.
 __device__ __forceinline__ int commit_init(Env& E, int v) {
@@ -1363,6 +1569,7 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
   E.st = p.st;
   E.variant = DC_HB;  // the prior-filtered mex of HB
   E.CH = p.unit_slots;
+  E.CHp = p.unit_slots;
   E.my_scanned = 0;
   E.gid = nullptr;
   E.gpush = nullptr;

@@ -106,7 +106,9 @@ class Server:
         self.clock = clock
         self.sleep = sleep
 
-    def run(self, requests) -> RunStats:
+    def run(self, requests, t0: float | None = None) -> RunStats:
+        """Serves `requests` (arrival times in seconds after t0; t0 = now by
+        default) and fills in each one's completion time."""
         reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
         queues: dict[int, deque] = {}
         size_cache: dict[int, tuple] = {}
@@ -119,7 +121,8 @@ class Server:
 
         st = RunStats()
         nxt = 0
-        t0 = self.clock()
+        if t0 is None:
+            t0 = self.clock()
         remaining = len(reqs)
         while remaining:
             now = self.clock() - t0
@@ -150,6 +153,78 @@ class Server:
         if reqs:
             st.makespan = max(r.done for r in reqs) - reqs[0].arrival
         return st
+
+
+class LanedServer:
+    """Continuous batching over several lanes that run side by side on the
+    device.  Each lane is its own pool (its own stream, and a share of the
+    SMs for its persistent launches), holds a fixed subset of the graphs and
+    serves their requests with its own host thread under the `batched`
+    policy, so a long launch in one lane does not hold up the requests of
+    the others: requests that arrive while other lanes' launches are on the
+    device start as soon as their own lane is free, and the lanes' launches
+    overlap.  A graph's requests stay in arrival order within its lane, so
+    every graph gets the same sequence of batches, and the same colours, as
+    under the single-lane policies.
+
+    lanes: [(pool, {global graph id: lane-local graph id}, vertex_capacity,
+    pool_slots), ...]."""
+
+    def __init__(self, lanes, max_lines: int = 1 << 22, clock=time.perf_counter, sleep=time.sleep):
+        self.lanes = [(Server(pool, "batched", vcap, slots, max_lines=max_lines, clock=clock, sleep=sleep), gmap)
+                      for pool, gmap, vcap, slots in lanes]
+        self.clock = clock
+
+    def run(self, requests) -> RunStats:
+        import threading
+
+        parts = []
+        for srv, gmap in self.lanes:
+            mine = [r for r in requests if r.graph in gmap]
+            local = [Request(r.rid, gmap[r.graph], r.lines, r.arrival) for r in mine]
+            parts.append((srv, mine, local))
+        if sum(len(m) for _, m, _ in parts) != len(requests):
+            raise ValueError("a request names a graph that no lane holds")
+        results, errors = [None] * len(parts), []
+        t0 = self.clock()
+
+        def work(i, srv, local):
+            try:
+                results[i] = srv.run(local, t0=t0)
+            except BaseException as e:  # reported after every lane has stopped
+                errors.append(e)
+
+        threads = [threading.Thread(target=work, args=(i, srv, local)) for i, (srv, _, local) in enumerate(parts)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+        st = RunStats()
+        for (srv, mine, local), rs in zip(parts, results):
+            for r, l in zip(mine, local):
+                r.done, r.iterations, r.launch = l.done, l.iterations, l.launch
+            st.launches += rs.launches
+            st.lines += rs.lines
+            st.device_ms += rs.device_ms
+            st.per_launch_requests += rs.per_launch_requests
+        done = [r for r in requests if r.done == r.done]
+        if done:
+            st.makespan = max(r.done for r in done) - min(r.arrival for r in requests)
+        return st
+
+
+def assign_lanes(sizes, lanes: int):
+    """Graph -> lane, balancing the lanes' total vertices (largest graphs
+    first, each to the lightest lane)."""
+    load = [0] * lanes
+    out = {}
+    for g in sorted(range(len(sizes)), key=lambda g: -sizes[g]):
+        j = min(range(lanes), key=lambda x: load[x])
+        out[g] = j
+        load[j] += sizes[g]
+    return out
 
 
 def make_trace(count: int, ngraphs: int, rate: float, seed: int, kmin: int = 10, kmax: int = 1_000_000,

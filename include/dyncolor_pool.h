@@ -50,7 +50,8 @@ typedef struct {
   int64_t pool_slots_max;  /* hard limit: when the graphs of one launch alone outgrow pool_slots, the
                               pool grows up to this many slots (and shrinks back at the next
                               compaction that allows it); <= 0: 2 * pool_slots */
-  int32_t reserved[8];
+  int32_t grid_ctas;       /* CTAs of the persistent launches (dc_options.grid_ctas); 0: all */
+  int32_t reserved[7];
 } dc_pool_options;
 
 /* One update batch for one graph. */

@@ -334,6 +334,10 @@ def test_heavy_row_index_matches_oracle(variant, ov, min_live, unit_slots):
     assert ctx.validate() == 0
     if min_live > 0:
         assert read < scanned
-    else:
+    elif variant == dc.HI:
         assert read == scanned
+    else:
+        # HB pulls the marks of a dense frontier: it may read fewer entries
+        # than the rule covers even without the index
+        assert read <= scanned
     ctx.close()

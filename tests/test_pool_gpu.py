@@ -180,3 +180,47 @@ def test_pool_grows_past_budget_only_for_one_launch_and_shrinks_back():
     assert np.array_equal(pool.colors(g1), scol)
     assert np.array_equal(pool.colors(g0), o.colors())
     pool.close()
+
+
+@pytest.mark.parametrize("variant,ov", [(dc.HI, po.HI), (dc.HB, po.HB)])
+def test_lanes_serve_overlapping_requests_like_each_graph_alone(variant, ov):
+    """Requests that arrive while other lanes' launches run: three pools side
+    by side (each with a third of the persistent CTAs, its own stream and a
+    host thread), continuous batching in each.  Every graph ends with the
+    colours, and every request with the iteration count, of applying the
+    graph's batches alone and in order."""
+    import torch
+
+    from dyncolor_b200.serve import LanedServer, Request, assign_lanes
+
+    graphs, colors, seqs = make_workload(12, seed=8, rounds=3)
+    want = oracle_runs(graphs, colors, seqs, ov)
+    sizes = [n for n, _, _ in graphs]
+    which = assign_lanes(sizes, 3)
+    ctas = max(1, 2 * torch.cuda.get_device_properties(0).multi_processor_count // 3)
+    lanes = []
+    for j in range(3):
+        gl = [g for g in range(len(graphs)) if which[g] == j]
+        nmax = max(sizes[g] for g in gl)
+        slots = sum(int(2.5 * len(graphs[g][1])) + 8 * sizes[g] for g in gl) + 4096
+        pool = ResidentPool(variant=variant, vertex_capacity=2 * sum(sizes[g] for g in gl) + nmax, pool_slots=slots,
+                            max_graphs=len(gl) + 1, grid_ctas=ctas, cuda_graph=True)
+        for g in gl:
+            n, a, b = graphs[g]
+            pool.add_graph(n, a, b, colors[g])
+        lanes.append((pool, {g: i for i, g in enumerate(gl)}, 2 * sum(sizes[g] for g in gl) + nmax, slots))
+    # all requests arrive at once, graph by graph round-robin, in batch order
+    reqs, rid = [], 0
+    for r in range(3):
+        for g in range(len(graphs)):
+            reqs.append(Request(rid, g, seqs[g][r], 1e-4 * rid))
+            rid += 1
+    st = LanedServer(lanes).run(reqs)
+    assert st.lines == sum(len(x) for s_ in seqs for x in s_)
+    for g in range(len(graphs)):
+        pool, gmap, _, _ = lanes[which[g]]
+        assert np.array_equal(pool.colors(gmap[g]), want[g][0]), f"graph {g}"
+        its = [r.iterations for r in sorted((r for r in reqs if r.graph == g), key=lambda r: r.rid)]
+        assert its == want[g][1], f"graph {g}"
+    for pool, _, _, _ in lanes:
+        pool.close()

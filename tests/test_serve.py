@@ -118,3 +118,59 @@ def test_trace_shape():
     assert top[0] > 0.12 * len(g1) and top[0] > 10 * top[50]  # Zipf(1.1)
     gaps = np.diff(arr)
     assert abs(gaps.mean() - 1e-3) < 5e-5
+
+
+class SleepPool(FakePool):
+    """A launch takes (real) time: 1 ms plus 20 ns per line, spent in
+    time.sleep, which lets other lanes' threads run meanwhile."""
+
+    def __init__(self, sizes):
+        super().__init__(None, sizes)
+
+    def apply(self, batch):
+        import time
+
+        graphs = [g for g, _ in batch]
+        assert len(set(graphs)) == len(graphs), "two batches for one graph in a launch"
+        lines = sum(len(x) for _, x in batch)
+        dt = 1e-3 + 2e-8 * lines
+        time.sleep(dt)
+        self.busy = getattr(self, "busy", 0.0) + dt
+        self.launches.append(batch)
+        for g, x in batch:
+            self.per_graph[g].append(int(x["node1"][0]) if len(x) else -1)
+        return FakeStats(1.0), np.arange(len(batch)), np.zeros(len(batch), np.int32)
+
+
+def test_lanes_overlap_and_keep_each_graphs_order():
+    from dyncolor_b200.serve import LanedServer, assign_lanes
+
+    ng = 24
+    sizes = [(100 + 10 * g, 1000) for g in range(ng)]
+
+    def lanes_run(nl):
+        which = assign_lanes([n for n, _ in sizes], nl)
+        lanes = []
+        for j in range(nl):
+            gl = sorted(g for g in range(ng) if which[g] == j)
+            gmap = {g: i for i, g in enumerate(gl)}
+            pool = SleepPool([sizes[g] for g in gl])
+            lanes.append((pool, gmap, 10_000, 1 << 20))
+        reqs = trace(240, ng, rate=100_000)
+        st = LanedServer(lanes, max_lines=4_000).run(reqs)
+        return st, reqs, lanes, which
+
+    st1, r1, lanes1, _ = lanes_run(1)
+    st4, r4, lanes4, which = lanes_run(4)
+    assert sorted(set(which.values())) == [0, 1, 2, 3]
+    assert all(r.done >= r.arrival for r in r4) and st4.lines == st1.lines
+    # every graph saw its requests in arrival order, in its own lane
+    for g in range(ng):
+        pool, gmap, _, _ = lanes4[which[g]]
+        tags = pool.per_graph[gmap[g]]
+        assert tags == sorted(tags) and len(tags) == sum(1 for r in r4 if r.graph == g)
+    # the four lanes' launches overlap: together they were busy for much
+    # longer than the run took
+    busy = sum(getattr(pool, "busy", 0.0) for pool, _, _, _ in lanes4)
+    assert busy > 1.5 * st4.makespan
+    assert st4.makespan < st1.makespan
