@@ -892,7 +892,9 @@ def run_served(args):
         for j in range(nl):
             gl = [g for g in range(len(graphs)) if which[g] == j]
             share = sum(sizes[g] for g in gl) / max(nsum, 1)
-            lv = max(int(vcap * share) + 2 * max(sizes[g] for g in gl), 2 * max(sizes[g] for g in gl))
+            # vertex ids are cheap next to rows: every graph of the lane keeps
+            # its ids, and the row budget alone decides what spills
+            lv = sum(sizes[g] for g in gl) + 2 * max(sizes[g] for g in gl)
             ls = max(int(slots * share * 1.2), 4 * max(int(2.5 * len(graphs[g][1])) + 4 * sizes[g] for g in gl))
             pool = ResidentPool(variant=variant, vertex_capacity=lv, pool_slots=ls, pool_slots_max=4 * ls,
                                 max_graphs=len(gl) + 1, cuda_graph=True,

@@ -76,7 +76,7 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     const bool hi = ctx->opt.variant == DC_HI;
     HriBufs& h = ctx->hri;
     h.min_live = ctx->opt.heavy_min_live;
-    h.cap_rows = ctx->pool_cap / h.min_live + 1;
+    h.cap_rows = std::min<long long>(n + 1, ctx->pool_cap / h.min_live + 1);
     h.cap_pairs = ctx->pool_cap / 4 + 4096;  // R-MAT scale 24: rows >= 2048 hold 236 M of 1.57 G slots
     h.cap_exc = hi ? h.cap_pairs : 1;       // a row's change list holds at most its live neighbours
     h.cap_a = hi ? n / 8 + ctx->pool_cap / 512 + 1024 : 1;  // items of 512 slots
@@ -406,8 +406,13 @@ dc_status enqueue_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const
     DC_CK(cudaMemsetAsync(reinterpret_cast<char*>(ctx->st) + b0, 0, b1 - b0, ctx->stream));
     RecolorParams rp = recolor_params(ctx, d_ch, k);
     rp.k_dev = k_dev;
-    if (ctx->use_index)
-      DC_CK(launch_hri_build(graph_dev(ctx), ctx->hri, ctx->st, ctx->opt.variant, ctx->stream));
+    rp.ranges = ctx->index_n > 0 ? ctx->d_ranges : nullptr;
+    if (ctx->use_index) {
+      HriBufs hb = ctx->hri;
+      hb.ranges = ctx->index_n > 0 ? ctx->d_ranges : nullptr;
+      rp.hri.ranges = hb.ranges;
+      DC_CK(launch_hri_build(graph_dev(ctx), hb, ctx->st, ctx->opt.variant, ctx->stream));
+    }
     else
       rp.hri.min_live = 0;  // this batch scans every row
     DC_CK(launch_recolor(rp, ctx->grid_recolor, ctx->stream));
@@ -428,7 +433,8 @@ void drop_graph(dc_ctx* ctx) {
 // into a CUDA graph; recaptured whenever a buffer it names was reallocated.
 dc_status ensure_graph(dc_ctx* ctx) {
   const long long key[6] = {ctx->kcap, ctx->k_pool_cap, ctx->rc_pool_cap, ctx->ngraphs,
-                            (long long)(uintptr_t)ctx->d_ch, ctx->use_index ? 1 : 0};
+                            (long long)(uintptr_t)ctx->d_ch,
+                            (ctx->use_index ? 1 : 0) + (ctx->index_n > 0 ? 2 : 0)};
   if (ctx->gexec && std::memcmp(key, ctx->graph_key, sizeof(key)) == 0) return DC_OK;
   drop_graph(ctx);
   DC_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
@@ -460,7 +466,8 @@ dc_status run_batch(dc_ctx* ctx, const dc_change* d_ch, const int* la, const int
   // launch; it pays off when the batch is large enough to start long
   // cascades through those rows, and a small batch on a big graph (or one
   // graph's batch in a pool of many) would mostly pay for the build.
-  ctx->use_index = recolor && ctx->hri.min_live > 0 && k * kIndexBatchRatio >= (long long)ctx->n;
+  ctx->use_index = recolor && ctx->hri.min_live > 0 &&
+                   k * kIndexBatchRatio >= (ctx->index_n > 0 ? ctx->index_n : (long long)ctx->n);
   bool compacted = false;
   for (int attempt = 0;; ++attempt) {
     const bool graph = ctx->opt.cuda_graph && recolor && attempt == 0;
@@ -688,6 +695,7 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->hri.alist);
   dfree(ctx, &ctx->hri.hist);
   dfree(ctx, &ctx->hri.hsplit);
+  dfree(ctx, &ctx->d_ranges);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->len);
   dfree(ctx, &ctx->cap);

@@ -99,6 +99,9 @@ struct dc_ctx {
   cudaGraphExec_t gexec = nullptr;
   long long graph_key[6] = {0, 0, 0, 0, 0, 0};
   bool use_index = false;  // this batch builds and uses the heavy-row index
+  int* d_ranges = nullptr;  // vertex ranges of the next batch's index (HriBufs::ranges), or unused
+  long long ranges_cap = 0; // ints
+  long long index_n = 0;    // > 0: the next batch's index covers d_ranges' vertices, this many
   long long* h_k = nullptr;  // pinned line count for the captured graph
   bool last_graph = false;   // the last batch ran from the captured graph
 

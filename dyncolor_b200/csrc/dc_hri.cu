@@ -27,23 +27,42 @@ __device__ __forceinline__ int hri_bin(int c) { return c < kHriBins - 1 ? c : kH
 // list once per launch (at its first colour change), so it never overflows.
 __device__ __forceinline__ long long xcap(int live) { return live; }
 
+__device__ __forceinline__ void classify_one(const GraphDev& g, const HriBufs& h, DevState* st, int v) {
+  int id = -1;
+  if (g.live[v] >= h.min_live) {
+    const unsigned long long i = atomicAdd(&st->hcount, 1ull);
+    if ((long long)i < h.cap_rows) {
+      id = (int)i;
+      h.hrow[i] = v;
+    }
+  }
+  h.hid[v] = id;
+}
+
 __global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
   const long long nt = (long long)gridDim.x * blockDim.x;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  for (long long v = t; v < g.n; v += nt) {
-    int id = -1;
-    if (g.live[v] >= h.min_live) {
-      const unsigned long long i = atomicAdd(&st->hcount, 1ull);
-      if ((long long)i < h.cap_rows) {
-        id = (int)i;
-        h.hrow[i] = (int)v;
-      }
+  if (!h.ranges) {
+    for (long long v = t; v < g.n; v += nt) classify_one(g, h, st, (int)v);
+    if (h.bmF) {
+      const long long words = ((long long)g.n + 31) / 32 + 1;
+      for (long long w = t; w < words; w += nt) h.bmF[w] = 0u;
     }
-    h.hid[v] = id;
+    return;
   }
-  if (h.bmF) {
-    const long long words = ((long long)g.n + 31) / 32 + 1;
-    for (long long w = t; w < words; w += nt) h.bmF[w] = 0u;
+  // the ranges' vertices, as one index space (binary search for the range)
+  const int cnt = h.ranges[0];
+  const long long total = h.ranges[1];
+  const int* r = h.ranges + 2;  // (first vertex, vertices before) per range
+  for (long long x = t; x < total; x += nt) {
+    int lo = 0, hi = cnt - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if ((long long)r[2 * mid + 1] <= x) lo = mid; else hi = mid - 1;
+    }
+    const int v = r[2 * lo] + (int)(x - r[2 * lo + 1]);
+    classify_one(g, h, st, v);
+    if (h.bmF) atomicAnd(&h.bmF[v >> 5], ~(1u << (v & 31)));
   }
 }
 
@@ -202,6 +221,7 @@ cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, 
   if (h.min_live <= 0 || g.n <= 0) return cudaSuccess;
   long long b = ((long long)g.n + kHriThreads - 1) / kHriThreads;
   if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
   hri_classify_kernel<<<(unsigned)b, kHriThreads, 0, s>>>(g, h, st);
   hri_offsets_kernel<<<1, kHriThreads, 0, s>>>(g, h, st);
   if (variant == DC_HB)

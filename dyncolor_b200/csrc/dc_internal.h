@@ -174,6 +174,12 @@ struct HriBufs {
                               // of them, then the rest
   long long cap_rows, cap_pairs, cap_exc, cap_a, cap_hist;
   int min_live;               // 0: no index
+  // Vertex ranges the index covers (nullptr: every vertex): [count, total,
+  // then per range its first vertex and the vertices before it in the
+  // ranges' concatenation].  A resident pool's launch touches only its own
+  // graphs, so their rows alone are indexed; hid of other vertices is never
+  // read during that launch.
+  const int* ranges;
 };
 
 struct RecolorParams {
@@ -194,6 +200,7 @@ struct RecolorParams {
   HriBufs hri;             // HI: heavy-row index (hri.min_live == 0: off)
   unsigned char* lflag;  // k
   int* pred;             // initial colouring: neighbours still to be coloured before each vertex
+  const int* ranges;     // vertex ranges of the launch's graphs (HriBufs::ranges layout), nullptr: all
   // Batched mode: the graph is a disjoint union of independent graphs.
   const int* gid;        // vertex -> graph (nullptr: one graph)
   int ngraphs;

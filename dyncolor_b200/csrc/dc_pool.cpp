@@ -79,6 +79,7 @@ struct dc_pool {
   dc_change* h_lines = nullptr;   // pinned union batch
   long long lines_cap = 0;
   int* h_giters = nullptr;        // pinned, G + 1
+  int* h_ranges = nullptr;        // pinned: the index ranges of a launch (HriBufs::ranges)
   std::unordered_map<void*, long long> hsizes;
   long long host_bytes = 0;
   long long budget = 0;  // adjacency slots for the packed rows of resident graphs
@@ -498,9 +499,8 @@ dc_status dc_pool_create(dc_pool** out, const dc_pool_options* opt) {
   dc_pool* P = new (std::nothrow) dc_pool();
   if (!P) return DC_E_NOMEM;
   P->opt = o;
-  // one launch serves a few of many resident graphs: an index rebuilt for
-  // the heavy rows of every resident graph would cost more than it saves
-  co.heavy_min_live = -1;
+  // a launch builds the heavy-row index over its own graphs' rows only
+  co.heavy_min_live = o.heavy_min_live;
   dc_status s = dc_create(&P->u, &co);
   if (s != DC_OK) {
     delete P;
@@ -532,6 +532,9 @@ dc_status dc_pool_create(dc_pool** out, const dc_pool_options* opt) {
   if ((s = dalloc(ctx, &P->d_pre, kChunkVertices + 1, "pool chunk offsets")) != DC_OK) return bail(s);
   if ((s = halloc(P, &P->h_prerel, kChunkVertices + 1)) != DC_OK) return bail(s);
   if ((s = halloc(P, &P->h_giters, G1)) != DC_OK) return bail(s);
+  if ((s = halloc(P, &P->h_ranges, 2 * G1 + 2)) != DC_OK) return bail(s);
+  if ((s = dalloc(P->u, &P->u->d_ranges, 2 * G1 + 2, "index ranges")) != DC_OK) return bail(s);
+  P->u->ranges_cap = 2 * G1 + 2;
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return bail(DC_E_CUDA);
   P->freemap[0] = o.vertex_capacity;
   *out = P;
@@ -560,6 +563,7 @@ void dc_pool_destroy(dc_pool* P) {
   hfree(P, &P->h_cap);
   hfree(P, &P->h_lines);
   hfree(P, &P->h_giters);
+  hfree(P, &P->h_ranges);
   if (P->u) dc_destroy(P->u);
   delete P;
 }
@@ -723,6 +727,22 @@ dc_status dc_pool_apply(dc_pool* P, const dc_pool_request* reqs, int32_t count, 
     w += r.k;
   }
   if (K > 0) {
+    // the launch's graphs: the only rows its heavy-row index needs
+    {
+      int* r = P->h_ranges;
+      long long tot = 0;
+      r[0] = count;
+      for (int32_t i = 0; i < count; ++i) {
+        const PGraph& g = P->graphs[(size_t)reqs[i].graph];
+        r[2 + 2 * i] = g.first;
+        r[3 + 2 * i] = (int)tot;
+        tot += g.n;
+      }
+      r[1] = (int)tot;
+      DC_CK(cudaMemcpyAsync(ctx->d_ranges, r, (size_t)(2 + 2 * count) * sizeof(int), cudaMemcpyHostToDevice,
+                            ctx->stream));
+      ctx->index_n = std::max<long long>(tot, 1);
+    }
     for (;;) {
       s = dc_apply_batch(ctx, P->h_lines, K, stats);
       if (s != DC_E_NOMEM) break;

@@ -45,10 +45,16 @@ namespace {
 
 enum Mode { M_MEX_ALL = 0, M_MEX_PRIOR = 1, M_DISTINCT = 2 };
 
+constexpr int kCtaBuf = 4096;  // vertices a CTA stages for the next queue during a find-eligible phase
+
 struct Shared {
   unsigned mask[kWarps][kMaskWords];  // per-warp colour window
   int pbuf[kWarps][64];               // per-warp buffer of newly marked vertices
   long long swll[kWarps];
+  int cbuf[kCtaBuf];                  // the CTA's newly marked vertices, pushed at the end of the phase
+  int ccnt;                           // entries claimed in cbuf (may pass kCtaBuf)
+  int sw[kWarps + 1];                 // block-scan scratch
+  unsigned long long qbase[2];        // queue positions the CTA's bulk push got (items, units)
 };
 
 __device__ __forceinline__ long long grab(unsigned long long* ctr) {
@@ -56,6 +62,30 @@ __device__ __forceinline__ long long grab(unsigned long long* ctr) {
   if (lane_id() == 0) x = atomicAdd(ctr, 1ull);
   return (long long)__shfl_sync(0xffffffffu, x, 0);
 }
+
+// Hands out the work items [0, total) of a phase to warps, `per` items per
+// atomic on the phase's counter: a counter takes one atomic at a time, so a
+// phase of hundreds of thousands of items would otherwise be bound by the
+// counter alone.  `per` grows with the items per warp (at most 32), keeping
+// the tail imbalance small.
+struct Grabber {
+  unsigned long long* ctr;
+  long long total, per, cur, end;
+  __device__ Grabber(unsigned long long* c, long long t, long long nwarps) : ctr(c), total(t), cur(0), end(0) {
+    per = t / (8 * nwarps);
+    per = per < 1 ? 1 : (per > 32 ? 32 : per);
+  }
+  // Warp-uniform.
+  __device__ __forceinline__ bool next(long long& i) {
+    if (cur >= end) {
+      cur = grab(ctr) * per;
+      if (cur >= total) return false;
+      end = min(total, cur + per);
+    }
+    i = cur++;
+    return true;
+  }
+};
 
 // Mask words a row of L slots needs in a colour window: the mex of at most
 // L colours is at most L, so colours >= min(L, kMaskBits) never matter;
@@ -161,6 +191,7 @@ struct Env {
   int variant;
   int CH;   // slots per work unit of the queue being processed
   int CHp;  // slots per work unit of the units this phase pushes
+  long long nwarps;  // warps of the grid
   long long my_scanned;
   // HB: (degree property << 32) | colour word per vertex, so one 8-byte
   // gather gives both; the next-frontier mark lives in its colour half
@@ -170,6 +201,8 @@ struct Env {
   bool hri_on;
   bool hri_mex;          // the loop's mex may use the index (its change lists are complete)
   bool hri_split;        // HB: indexed rows list their prior neighbours first
+  Shared* sh;            // the CTA's shared memory
+  bool cta_stage;        // flush() stages vertices in the CTA buffer (the phase ends with cta_push)
   long long read_delta;  // entries read minus entries the rules cover
   // batched mode (all nullptr for one graph)
   const int* gid;
@@ -536,9 +569,9 @@ __device__ void phase_reduce(Env& E, Shared& sh, const QueueBufs& qb, const QCou
   const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
   const long long nAb = (cA + 31) / 32;
   const long long total = cU + nAb;
-  while (true) {
-    const long long i = grab(ctr);
-    if (i >= total) break;
+  Grabber gb(ctr, total, E.nwarps);
+  long long i;
+  while (gb.next(i)) {
     if (i < cU)
       reduce_unit(E, sh, qb, qb.units[i], mode, out);
     else
@@ -578,15 +611,88 @@ struct PushBuf {
 };
 
 __device__ __forceinline__ void flush(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, int k) {
-  const int u = lane_id() < k ? pb.buf[lane_id()] : -1;
+  int u = lane_id() < k ? pb.buf[lane_id()] : -1;
   __syncwarp();
-  if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
-  warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CHp, &E.st->status);
+  if (E.cta_stage) {
+    // stage in the CTA buffer (one shared atomic); what does not fit goes
+    // to the queue directly
+    int base = 0;
+    if (lane_id() == 0) base = atomicAdd(&E.sh->ccnt, k);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (u >= 0 && base + lane_id() < kCtaBuf) {
+      E.sh->cbuf[base + lane_id()] = u;
+      u = -1;
+    }
+    if (__any_sync(0xffffffffu, u >= 0)) {
+      if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
+      warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CHp, &E.st->status);
+    }
+  } else {
+    if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
+    warp_push(nq, nc, E.g.len, u, true, M_MEX_ALL, E.CHp, &E.st->status);
+  }
   // keep the remainder at the front
   const int rest = pb.cnt - k;
   if (lane_id() < rest) pb.buf[lane_id()] = pb.buf[k + lane_id()];  // rest <= 31 < k
   __syncwarp();
   pb.cnt = rest;
+}
+
+// Pushes the CTA buffer into the queue after every warp of the CTA has
+// finished the phase: one pair of queue atomics for the whole CTA (block
+// scans of the class-A items and of the work units), then every thread
+// writes its entries.  All threads of the CTA call it.
+__device__ void cta_push(Env& E, const QueueBufs& qb, QCount* qc) {
+  Shared& sh = *E.sh;
+  __syncthreads();
+  const int cnt = min(sh.ccnt, kCtaBuf);
+  const int CH = E.CHp;
+  for (int b0 = 0; b0 < cnt; b0 += kThreads) {
+    const int i = b0 + (int)threadIdx.x;
+    const int u = i < cnt ? sh.cbuf[i] : -1;
+    const int L = u >= 0 ? E.g.len[u] : 0;
+    const bool isA = u >= 0 && L <= kSmall;
+    const int c = (u >= 0 && !isA) ? (L > CH ? (L + CH - 1) / CH : 1) : 0;
+    if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
+    int totA = 0, totU = 0;
+    const int ea = block_excl_scan(isA ? 1 : 0, sh.sw, &totA);
+    const int eu = block_excl_scan(c, sh.sw, &totU);
+    if (threadIdx.x == 0 && totA) sh.qbase[0] = atomicAdd(&qc->countA, (unsigned long long)totA);
+    if (threadIdx.x == 32 && totU) sh.qbase[1] = atomicAdd(&qc->countU, (unsigned long long)totU);
+    __syncthreads();
+    if (isA) {
+      const unsigned long long pa = sh.qbase[0] + ea;
+      if ((long long)pa < qb.capA)
+        qb.itemsA[pa] = u;
+      else
+        atomicOr(&E.st->status, ST_OVERFLOW);
+    }
+    if (c > 0) {
+      int ms = -1;
+      bool ok = true;
+      if (c > 1) {
+        const int words = (mask_words(L, M_MEX_ALL) + 1 + 3) & ~3;
+        const unsigned long long mo = atomicAdd(&qc->masks, (unsigned long long)words);
+        if ((long long)(mo + words) > qb.capM) {
+          atomicOr(&E.st->status, ST_OVERFLOW);
+          ok = false;
+        } else {
+          uint4* m = reinterpret_cast<uint4*>(qb.gmask + mo);
+          for (int w = 0; w < words / 4; ++w) m[w] = make_uint4(0, 0, 0, 0);
+          ms = (int)mo;
+        }
+      }
+      const unsigned long long pu = sh.qbase[1] + eu;
+      for (int q = 0; ok && q < c; ++q) {
+        if ((long long)(pu + q) < qb.capU)
+          qb.units[pu + q] = make_int4(u, q, ms, c);
+        else
+          atomicOr(&E.st->status, ST_OVERFLOW);
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sh.ccnt = 0;
 }
 
 // The word that holds u's next-frontier mark: its colour word (HI) or the
@@ -610,6 +716,26 @@ __device__ __forceinline__ void claim(Env& E, PushBuf& pb, const QueueBufs& nq, 
   __syncwarp();
   pb.cnt += __popc(bal);
   if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
+}
+
+// claim() for four candidates per lane at once: their mark atomics are all
+// in flight before any result is used.  All lanes must call.
+__device__ __forceinline__ void claim4(Env& E, PushBuf& pb, const QueueBufs& nq, QCount* nc, const int* uu,
+                                       const bool* want, const unsigned* ww) {
+  unsigned old[4];
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    old[j] = (want[j] && !(ww[j] & kMarkBit)) ? atomicOr(mark_word(E, uu[j]), kMarkBit) : kMarkBit;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const bool got = !(old[j] & kMarkBit);
+    const unsigned bal = __ballot_sync(0xffffffffu, got);
+    if (!bal) continue;
+    if (got) pb.buf[pb.cnt + __popc(bal & lanemask_lt())] = uu[j];
+    __syncwarp();
+    pb.cnt += __popc(bal);
+    if (pb.cnt >= 32) flush(E, pb, nq, nc, 32);
+  }
 }
 
 // HI findEligibleNeighbors over one unit of an indexed row v: the unit's
@@ -652,8 +778,7 @@ __device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi
           const int cu = (int)(ww[j] & (unsigned)kColorMask);
           mu[j] = uu[j] >= 0 && ((R.cv == cu && R.v < uu[j]) || (R.pv < cu));
         }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
+        claim4(E, pb, nq, nc, uu, mu, ww);
         // the copy is in descending colour order: once a round ends below
         // both thresholds, so does the rest of the slice
         const int sl = (int)(H.pairs[min(r0 + 127, p1 - 1)] >> 32);
@@ -681,8 +806,7 @@ __device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi
         const int cu = (int)(ww[j] & (unsigned)kColorMask);
         mu[j] = uu[j] >= 0 && ((R.cv == cu && R.v < uu[j]) || (R.pv < cu));
       }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
+      claim4(E, pb, nq, nc, uu, mu, ww);
     }
   }
   if (lane_id() == 0) E.read_delta += reads - (p1 > p0 ? p1 - p0 : 0);
@@ -717,9 +841,9 @@ __device__ void phase_append(Env& E, unsigned long long* ctr) {
   // an overflowed queue has unwritten items, and the index is off anyway
   if (ld_cg(&E.st->hri_off) != 0u) return;
   const long long cnt = min((long long)ld_cg(&E.st->a_count), H.cap_a);
-  while (true) {
-    const long long i = grab(ctr);
-    if (i >= cnt) break;
+  Grabber gb(ctr, cnt, E.nwarps);
+  long long i;
+  while (gb.next(i)) {
     const int2 it = H.alist[i];
     const int v = it.x;
     const int chunk = it.y & ((1 << kChunkBits) - 1);
@@ -812,8 +936,7 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
       eligible(E, R, uu[j], cc[j], pp[j], &mu[j], &mv);
       markv |= mv;
     }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) claim(E, pb, nq, nc, uu[j], mu[j], ww[j]);
+    claim4(E, pb, nq, nc, uu, mu, ww);
   }
   const bool mv = __any_sync(0xffffffffu, markv);
   claim(E, pb, nq, nc, v, mv && lane_id() == 0, mv ? ld_cg(mark_word(E, v)) : kMarkBit);
@@ -861,15 +984,21 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
     }
 #pragma unroll
     for (int r = 0; r < 4; ++r) cc[r] = (int)(ww[r] & (unsigned)kColorMask);
+    bool mu[4], mv[4];
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
-      bool mu = false, mv = false;
+      mu[r] = false;
+      mv[r] = false;
       if (uu[r] >= 0) {
         ++E.my_scanned;
-        eligible(E, R[r], uu[r], cc[r], pp[r], &mu, &mv);
+        eligible(E, R[r], uu[r], cc[r], pp[r], &mu[r], &mv[r]);
       }
-      claim(E, pb, nq, nc, uu[r], mu, ww[r]);
-      claim(E, pb, nq, nc, R[r].v, mv, mv ? ld_cg(mark_word(E, R[r].v)) : kMarkBit);
+    }
+    claim4(E, pb, nq, nc, uu, mu, ww);
+    if (E.variant == DC_HB) {
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        claim(E, pb, nq, nc, R[r].v, mv[r], mv[r] ? ld_cg(mark_word(E, R[r].v)) : kMarkBit);
     }
   }
 }
@@ -883,15 +1012,16 @@ __device__ void phase_expand(Env& E, Shared& sh, const QueueBufs& fq, const QCou
   PushBuf pb;
   pb.buf = sh.pbuf[warp_id()];
   pb.cnt = 0;
-  while (true) {
-    const long long i = grab(ctr);
-    if (i >= total) break;
+  Grabber gb(ctr, total, E.nwarps);
+  long long i;
+  while (gb.next(i)) {
     if (i < cU)
       expand_unit(E, pb, fq.units[i], nq, nc);
     else
       expand_batchA(E, pb, fq, cA, i - cU, nq, nc);
   }
   if (pb.cnt > 0) flush(E, pb, nq, nc, pb.cnt);
+  if (E.cta_stage) cta_push(E, nq, nc);
 }
 
 // ---------------------------------------------------------------------
@@ -959,9 +1089,19 @@ __device__ void phase_mark_frontier(Env& E, const QueueBufs& fq, const QCount* f
 
 __device__ __forceinline__ bool in_bits(const unsigned* bm, int v) { return (ld_cg(&bm[v >> 5]) >> (v & 31)) & 1u; }
 
-// Walks u's neighbours prior to u (an indexed row lists them first) until
-// one is in the frontier, or -- when u is in the frontier -- has u's colour.
-// One lane.
+// Index of u's heavy row, or -1.  Checked against the row list, because a
+// pool launch indexes its own graphs' rows only and the entries of other
+// vertices are left from earlier launches.
+__device__ __forceinline__ int heavy_row(const Env& E, int u) {
+  const int hi = E.hri.hid[u];
+  if (hi < 0 || hi >= E.hri.cap_rows || (unsigned long long)hi >= ld_cg(&E.st->hcount)) return -1;
+  return E.hri.hrow[hi] == u ? hi : -1;
+}
+
+// Walks u's neighbours until one prior to u is in the frontier, or -- when
+// u is in the frontier -- has u's colour.  One lane, four neighbours per
+// step (their ids, then their packed words, then their membership bits, each
+// four loads in flight).
 __device__ __forceinline__ bool pull_lane(const Env& E, const unsigned* inF, int u, long long& reads) {
   const GraphDev& g = E.g;
   const int L = g.len[u];
@@ -969,13 +1109,22 @@ __device__ __forceinline__ bool pull_lane(const Env& E, const unsigned* inF, int
   const int pu = g.prop[u];
   const bool fu = in_bits(inF, u);
   const int cu = (int)((unsigned)E.cp[u] & (unsigned)kColorMask);
-  for (int s = 0; s < L; ++s) {
-    const int w = g.adj[o + s];
-    if (w < 0) continue;
-    ++reads;
-    const unsigned long long x = E.cp[w];
-    if (!is_prior((int)(x >> 32), w, pu, u)) continue;
-    if (in_bits(inF, w) || (fu && (int)((unsigned)x & (unsigned)kColorMask) == cu)) return true;
+  for (int s0 = 0; s0 < L; s0 += 4) {
+    int w[4];
+    unsigned long long x[4];
+    bool pr[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) w[j] = s0 + j < L ? g.adj[o + s0 + j] : -1;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) x[j] = w[j] >= 0 ? E.cp[w[j]] : 0ull;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      pr[j] = w[j] >= 0 && is_prior((int)(x[j] >> 32), w[j], pu, u);
+      reads += w[j] >= 0;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (pr[j] && (in_bits(inF, w[j]) || (fu && (int)((unsigned)x[j] & (unsigned)kColorMask) == cu))) return true;
   }
   return false;
 }
@@ -986,7 +1135,7 @@ __device__ bool pull_warp(const Env& E, const unsigned* inF, int u, long long& r
   const int pu = g.prop[u];
   const bool fu = in_bits(inF, u);
   const int cu = (int)((unsigned)E.cp[u] & (unsigned)kColorMask);
-  const int hi = E.hri_split ? E.hri.hid[u] : -1;
+  const int hi = E.hri_split ? heavy_row(E, u) : -1;
   if (hi >= 0) {
     // prior neighbours first: only they can mark u
     const long long pb = E.hri.hoff[hi];
@@ -1021,21 +1170,36 @@ __device__ bool pull_warp(const Env& E, const unsigned* inF, int u, long long& r
   return false;
 }
 
-// Every vertex decides whether it joins the next frontier; lanes take rows
-// of up to kPullLane slots, the warp then takes the longer rows of its 32
-// vertices one by one.
-__device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const QueueBufs& nq, QCount* nc,
-                              long long gwarp, long long nwarps) {
+// Every vertex of the launch's graphs (all vertices, or the vertex ranges
+// of a pool launch) decides whether it joins the next frontier; lanes take
+// rows of up to kPullLane slots, the warp then takes the longer rows of its
+// 32 vertices one by one.
+__device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const int* ranges, const QueueBufs& nq,
+                              QCount* nc, long long gwarp, long long nwarps) {
   const GraphDev& g = E.g;
   PushBuf pb;
   pb.buf = sh.pbuf[warp_id()];
   pb.cnt = 0;
   long long reads = 0;
-  for (long long b0 = gwarp * 32; b0 < g.n; b0 += nwarps * 32) {
-    const long long ul = b0 + lane_id();
-    int u = ul < g.n ? (int)ul : -1;
+  const long long total = ranges ? (long long)ranges[1] : (long long)g.n;
+  for (long long b0 = gwarp * 32; b0 < total; b0 += nwarps * 32) {
+    const long long x = b0 + lane_id();
+    int u = -1;
+    if (x < total) {
+      if (ranges) {
+        const int* r = ranges + 2;
+        int lo = 0, hi = ranges[0] - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) / 2;
+          if ((long long)r[2 * mid + 1] <= x) lo = mid; else hi = mid - 1;
+        }
+        u = r[2 * lo] + (int)(x - r[2 * lo + 1]);
+      } else {
+        u = (int)x;
+      }
+    }
     if (u >= 0 && E.gskip && ld_cg(&E.gskip[E.gid[u]]) == 0) u = -1;  // its graph has stopped
-    const bool lng = u >= 0 && (g.len[u] > kPullLane || (E.hri_split && E.hri.hid[u] >= 0));
+    const bool lng = u >= 0 && (g.len[u] > kPullLane || (E.hri_split && heavy_row(E, u) >= 0));
     bool want = false;
     if (u >= 0 && !lng) want = pull_lane(E, inF, u, reads);
     push_ready(E, pb, nq, nc, u, want);
@@ -1043,16 +1207,17 @@ __device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const Que
     while (todo) {
       const int l = __ffs(todo) - 1;
       todo &= todo - 1;
-      const int x = __shfl_sync(0xffffffffu, u, l);
+      const int v = __shfl_sync(0xffffffffu, u, l);
       long long r = 0;
-      const bool m = pull_warp(E, inF, x, r);
+      const bool m = pull_warp(E, inF, v, r);
       if (lane_id() == 0) reads += r;
-      push_ready(E, pb, nq, nc, x, m && lane_id() == 0);
+      push_ready(E, pb, nq, nc, v, m && lane_id() == 0);
     }
   }
   if (pb.cnt > 0) flush(E, pb, nq, nc, pb.cnt);
   reads = warp_sum_ll(reads);
   if (lane_id() == 0) E.read_delta += reads;
+  if (E.cta_stage) cta_push(E, nq, nc);
 }
 
 __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int kind,
@@ -1172,6 +1337,10 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
   E.hri_mex = false;  // set once the seeding's changes are in the change lists
   E.hri_split = V == DC_HB && p.hri.min_live > 0;
   E.read_delta = 0;
+  E.sh = &sh;
+  E.cta_stage = false;
+  E.nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+  if (threadIdx.x == 0) sh.ccnt = 0;
   DevState* st = p.st;
   const GraphDev& g = E.g;
   unsigned bar = 0;
@@ -1378,17 +1547,19 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         E.CHp = unit_slots_for(items, nwarps, p.unit_slots);
         if (leader) st->q[ns].ch = (unsigned long long)E.CHp;
       }
-      // HB with a frontier of more than a sixteenth of the vertices pulls
-      const bool pull = V == DC_HB &&
-                        (long long)(ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU)) * 16 > (long long)g.n;
+      // HB with a frontier of more than a sixteenth of the launch's vertices pulls
+      const bool pull = V == DC_HB && (long long)(ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU)) * 16 >
+                                          (p.ranges ? (long long)p.ranges[1] : (long long)g.n);
+      E.cta_stage = true;
       if (pull) {
         phase_mark_frontier(E, p.qb[fb], &st->q[fs], p.bmC, gwarp, nwarps);
         if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
-        phase_pull_hb(E, sh, p.bmC, p.qb[nb], &st->q[ns], gwarp, nwarps);
+        phase_pull_hb(E, sh, p.bmC, p.ranges, p.qb[nb], &st->q[ns], gwarp, nwarps);
       } else {
         phase_expand(E, sh, p.qb[fb], &st->q[fs], p.qb[nb], &st->q[ns], ctr());
         ++ps;
       }
+      E.cta_stage = false;
       if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       lap(1);
       const QCount* nc = &st->q[ns];
@@ -1582,6 +1753,9 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
   E.hri_mex = false;
   E.hri_split = false;
   E.read_delta = 0;
+  E.sh = &sh;
+  E.cta_stage = false;
+  E.nwarps = (long long)gridDim.x * (blockDim.x >> 5);
   DevState* st = p.st;
   const GraphDev& g = E.g;
   int* pred = p.pred;
@@ -1613,10 +1787,9 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
     const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
     const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
     const long long total = cU + (cA + 31) / 32;
-    unsigned long long* c = ctr();
-    while (true) {
-      const long long i = grab(c);
-      if (i >= total) break;
+    Grabber gb(ctr(), total, E.nwarps);
+    long long i;
+    while (gb.next(i)) {
       if (i < cU)
         pred_unit(E, qb.units[i], pred);
       else
@@ -1663,10 +1836,9 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
       PushBuf pb;
       pb.buf = sh.pbuf[warp_id()];
       pb.cnt = 0;
-      unsigned long long* c = ctr();
-      while (true) {
-        const long long i = grab(c);
-        if (i >= total) break;
+      Grabber gb(ctr(), total, E.nwarps);
+      long long i;
+      while (gb.next(i)) {
         if (i < cU)
           release_unit(E, pb, fq.units[i], pred, p.qb[nb], &st->q[ns], cmax);
         else

@@ -32,7 +32,8 @@ class PoolOptions(C.Structure):
         ("stage_slots", C.c_int64),
         ("pool_slots_max", C.c_int64),
         ("grid_ctas", C.c_int32),
-        ("reserved", C.c_int32 * 7),
+        ("heavy_min_live", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 
@@ -105,7 +106,8 @@ class ResidentPool:
     def __init__(self, variant: int = HI, vertex_capacity: int = 1 << 22, pool_slots: int = 1 << 28,
                  max_graphs: int = 1024, device: int = 0, iter_cap: int = 0, slack: float = 0.0,
                  blocks_per_sm: int = 0, unit_slots: int = 0, cuda_graph: bool = False,
-                 stage_slots: int = 0, pool_slots_max: int = 0, stream: int = 0, grid_ctas: int = 0):
+                 stage_slots: int = 0, pool_slots_max: int = 0, stream: int = 0, grid_ctas: int = 0,
+                 heavy_min_live: int = 0):
         L = _lib()
         o = PoolOptions()
         L.dc_pool_options_default(C.byref(o))
@@ -127,6 +129,7 @@ class ResidentPool:
             o.stage_slots = stage_slots
         o.pool_slots_max = pool_slots_max
         o.grid_ctas = grid_ctas
+        o.heavy_min_live = heavy_min_live
         h = C.c_void_p()
         rc = L.dc_pool_create(C.byref(h), C.byref(o))
         if rc != OK:

@@ -51,14 +51,18 @@ def oracle_runs(graphs, colors, seqs, ov):
 
 
 @pytest.mark.parametrize("variant,ov", [(dc.HI, po.HI), (dc.HB, po.HB)])
-def test_pool_spill_reload_and_shared_launches_match_alone(variant, ov):
+@pytest.mark.parametrize("heavy_min_live", [-1, 64])
+def test_pool_spill_reload_and_shared_launches_match_alone(variant, ov, heavy_min_live):
+    """With the heavy-row index off, and on from 64 live slots (each launch
+    then indexes the rows of its own graphs only, wherever the pool placed
+    them, after other graphs used and left those vertex ids)."""
     graphs, colors, seqs = make_workload(10, seed=3)
     want = oracle_runs(graphs, colors, seqs, ov)
     nmax = max(n for n, _, _ in graphs)
     # room for about three graphs: every launch below forces evictions
     slots = int(3.2 * max(2 * len(a) for _, a, _ in graphs) * 1.25) + 64 * nmax
     pool = ResidentPool(variant=variant, vertex_capacity=3 * nmax, pool_slots=slots, max_graphs=16,
-                        unit_slots=256, stage_slots=4096)
+                        unit_slots=256, stage_slots=4096, heavy_min_live=heavy_min_live)
     ids = [pool.add_graph(n, a, b, c) for (n, a, b), c in zip(graphs, colors)]
     assert ids == list(range(len(graphs)))
     info = pool.info()
