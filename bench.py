@@ -74,6 +74,8 @@ def parse_args():
                     help="plain: one large graph (headline); batched: many graphs in one launch; "
                          "served: request stream over resident graphs")
     ap.add_argument("--graphs", type=int, default=4096, help="batched mode: number of graphs")
+    ap.add_argument("--default-batched-graphs", type=int, default=512,
+                    help="plain mode: graphs of the short batched comparison under detail.batched (0: none)")
     ap.add_argument("--served-graphs", type=int, default=256, help="served mode: resident graphs")
     ap.add_argument("--served-smin", type=int, default=14, help="served mode: smallest graph scale")
     ap.add_argument("--served-smax", type=int, default=20, help="served mode: largest graph scale")
@@ -86,6 +88,8 @@ def parse_args():
                     help="served mode: plain (one batch per launch), batched (continuous batching in one pool), "
                          "lanes (continuous batching in --lanes pools side by side)")
     ap.add_argument("--lanes", type=int, default=4, help="served mode: pools that run side by side")
+    ap.add_argument("--pool-heavy-min-live", type=int, default=0,
+                    help="served mode: the pools' heavy-row index threshold (<= 0: off, the library default)")
     return ap.parse_args()
 
 
@@ -657,6 +661,15 @@ def run_ours(args, dist: Dist):
         t0 = time.time()
         out["detail"]["configs"] = run_further_configs(args, w, dev, stream)
         out["detail"]["configs_s"] = round(time.time() - t0, 1)
+        if args.default_batched_graphs > 0:
+            # the batched configuration, shortened: graphs in one launch
+            # against each graph alone, every graph's colours compared
+            t0 = time.time()
+            b = run_batched(args, dist, count=args.default_batched_graphs, tune=False)
+            out["detail"]["batched"] = {k: b[k] for k in ("value", "unit", "ms_per_step", "e2e",
+                                                           "plain_each_graph_alone", "speedup_vs_plain",
+                                                           "bit_exact_vs_alone", "graphs_differing", "config")}
+            out["detail"]["batched_s"] = round(time.time() - t0, 1)
     return out, w, first_colors, first_stats
 
 
@@ -698,11 +711,15 @@ def build_batched_workload(count, seed, nmin=1_000, nmax=200_000, kmin=100, kmax
     return [o[0] for o in out], [o[1] for o in out], [o[2] for o in out]
 
 
-def run_batched(args, dist):
+def run_batched(args, dist, count=None, tune=True):
+    """Batched mode: `count` graphs (default --graphs) in one launch sequence
+    against each graph alone.  tune=False keeps the library's tile defaults
+    (the short comparison the default run reports under detail.batched)."""
     import dyncolor_b200 as dc
     from dyncolor_b200.batched import BatchedContext
     from dyncolor_b200.tune import autotune
 
+    count = args.graphs if count is None else count
     variant = dc.HI if args.variant == "hi" else dc.HB
     t0 = time.time()
     import torch
@@ -710,21 +727,23 @@ def run_batched(args, dist):
     torch.cuda.set_device(dist.local)
     dev = dist.local
     # whole graphs per GPU: rank r takes graphs r, r + N, ...
-    graphs, colors, batches = build_batched_workload(args.graphs, args.seed, rank=dist.rank, world=dist.world)
+    graphs, colors, batches = build_batched_workload(count, args.seed, rank=dist.rank, world=dist.world)
     gen_s = time.time() - t0
     lines = int(sum(len(x) for x in batches))
-    # autotune the tile parameters on a sample of the graphs
-    rng = np.random.default_rng(args.seed + 1)
-    idx = sorted(rng.choice(len(graphs), min(256, len(graphs)), replace=False).tolist())
-    sg, sc, sb = [graphs[i] for i in idx], [colors[i] for i in idx], [batches[i] for i in idx]
+    best, table = {}, {}
+    if tune:
+        # autotune the tile parameters on a sample of the graphs
+        rng = np.random.default_rng(args.seed + 1)
+        idx = sorted(rng.choice(len(graphs), min(256, len(graphs)), replace=False).tolist())
+        sg, sc, sb = [graphs[i] for i in idx], [colors[i] for i in idx], [batches[i] for i in idx]
 
-    def make(opts):
-        bc = BatchedContext(variant=variant, device=dev, **opts)
-        bc.load(sg)
-        bc.set_colors(sc)
-        return bc
+        def make(opts):
+            bc = BatchedContext(variant=variant, device=dev, **opts)
+            bc.load(sg)
+            bc.set_colors(sc)
+            return bc
 
-    best, table = autotune(make, lambda bc: bc.apply(sb).device_ms)
+        best, table = autotune(make, lambda bc: bc.apply(sb).device_ms)
     # all graphs, one launch (replayed from a captured CUDA graph)
     bc = BatchedContext(variant=variant, device=dev, cuda_graph=True, **best)
     bc.load(graphs)
@@ -771,7 +790,7 @@ def run_batched(args, dist):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": 1, "warmup": 0,
         "ms_per_step": dev_b, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
         "dtype": "int32", "data": "synthetic", "mode": "batched",
-        "config": {"workload": (f"{args.graphs} independent graphs (vertices log-uniform in [1k, 200k], "
+        "config": {"workload": (f"{count} independent graphs (vertices log-uniform in [1k, 200k], "
                                 f"average degree uniform in [8, 32], R-MAT / Erdos-Renyi alternating), one "
                                 f"batch per graph (log-uniform in [100, 50k] lines, 50/50), variant "
                                 f"{args.variant.upper()}"),
@@ -779,7 +798,7 @@ def run_batched(args, dist):
                    "parallelism": f"whole graphs per GPU over {dist.world} GPU(s)"},
         "e2e": {"value": lines / e2e_b, "unit": UNIT, "h2d_bytes_per_step": 12 * lines,
                 "d2h_bytes_per_step": 4 * nverts},
-        "plain_each_graph_alone": {"value": plain, "e2e": lines / e2e_p, "launches": 2 * args.graphs,
+        "plain_each_graph_alone": {"value": plain, "e2e": lines / e2e_p, "launches": 2 * count,
                                    "device_ms": dev_plain},
         "speedup_vs_plain": value / plain,
         "bit_exact_vs_alone": same, "graphs_differing": mismatched,
@@ -881,7 +900,8 @@ def run_served(args):
         budget."""
         if policy != "lanes":
             pool = ResidentPool(variant=variant, vertex_capacity=vcap, pool_slots=slots, pool_slots_max=4 * slots,
-                                max_graphs=len(graphs) + 1, cuda_graph=True)
+                                max_graphs=len(graphs) + 1, cuda_graph=True,
+                                heavy_min_live=args.pool_heavy_min_live)
             return [(pool, {g: g for g in range(len(graphs))}, vcap, slots)]
         nl = args.lanes
         which = assign_lanes(sizes, nl)
@@ -898,7 +918,8 @@ def run_served(args):
             ls = max(int(slots * share * 1.2), 4 * max(int(2.5 * len(graphs[g][1])) + 4 * sizes[g] for g in gl))
             pool = ResidentPool(variant=variant, vertex_capacity=lv, pool_slots=ls, pool_slots_max=4 * ls,
                                 max_graphs=len(gl) + 1, cuda_graph=True,
-                                grid_ctas=max(1, 2 * props.multi_processor_count // nl))
+                                grid_ctas=max(1, 2 * props.multi_processor_count // nl),
+                                heavy_min_live=args.pool_heavy_min_live)
             out.append((pool, {g: i for i, g in enumerate(gl)}, lv, ls))
         return out
 
@@ -944,8 +965,8 @@ def run_served(args):
             for pool, _, _, _ in lanes:
                 pool.close()
     top = [r for r in runs if r["offered_req_per_s"] == max(loads)]
-    best = max((r for r in top if r["policy"] != "plain"), key=lambda r: r["updates_per_s"])
-    plain = next(r for r in top if r["policy"] == "plain")
+    best = max(top, key=lambda r: (r["policy"] != "plain", r["updates_per_s"]))
+    plain = next((r for r in top if r["policy"] == "plain"), best)
     return {
         "metric": METRIC, "value": best["updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": len(runs),
         "warmup": 0, "ms_per_step": best["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",

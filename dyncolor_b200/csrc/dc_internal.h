@@ -40,7 +40,7 @@ struct QCount {
   unsigned long long countA;  // class A items
   unsigned long long countU;  // work units (class B/C)
   unsigned long long masks;   // multi-unit mask words handed out
-  unsigned long long ch;      // slots per work unit of the queue's units (0: unit_slots)
+  unsigned long long pad;
 };
 
 // Lives in device memory.  Fields up to `pool_used_start` persist across

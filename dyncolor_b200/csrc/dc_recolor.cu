@@ -97,6 +97,18 @@ __device__ __forceinline__ int mask_words(int L, int mode) {
   return min(kMaskWords, max(2, (limit + 31) / 32 + 1));
 }
 
+// Work units of a row: a row of L slots pushed with unit size CH is cut
+// into row_units(L, CH) units.  Consumers recover the span of every unit
+// from L and the unit count alone (the queue need not record CH): the units
+// split the row evenly, in multiples of 128 slots.  (Cutting hub rows into
+// quarter units as well was measured 21 % slower on the headline: the extra
+// units' mask combining costs more than the shorter units save.)
+__device__ __forceinline__ int row_units(int L, int CH) { return L > CH ? (L + CH - 1) / CH : 1; }
+__device__ __forceinline__ int unit_span(int L, int nch) {
+  const int s = (L + nch - 1) / nch;
+  return (s + 127) & ~127;
+}
+
 // Pushes u (or nothing when u < 0) into a queue.  Rows of more than one
 // unit get a global mask region [done counter, mask words...].  All 32 lanes
 // must call.
@@ -113,7 +125,7 @@ __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const
       atomicOr(status, ST_OVERFLOW);
   }
   int c = 0;
-  if (isU) c = L > CH ? (L + CH - 1) / CH : 1;
+  if (isU) c = row_units(L, CH);
   const unsigned long long pu = warp_atomic_add(&qc->countU, c);
   if (isU) {
     int ms = -1;
@@ -189,8 +201,8 @@ struct Env {
   GraphDev g;
   DevState* st;
   int variant;
-  int CH;   // slots per work unit of the queue being processed
-  int CHp;  // slots per work unit of the units this phase pushes
+  int CH;   // unit size of the seeding phases' pushes
+  int CHp;  // unit size of the units this phase pushes (row_units)
   long long nwarps;  // warps of the grid
   long long my_scanned;
   // HB: (degree property << 32) | colour word per vertex, so one 8-byte
@@ -306,8 +318,9 @@ __device__ bool reduce_heavy(Env& E, Shared& sh, const QueueBufs& qb, int4 un, i
   unsigned* sm = sh.mask[warp_id()];
   for (int k = lane_id(); k < nw; k += 32) sm[k] = 0;
   __syncwarp();
-  const long long e0 = (long long)un.y * E.CH;
-  const long long e1 = min((long long)xc, e0 + E.CH);
+  const int us = unit_span(E.g.len[v], nch);
+  const long long e0 = (long long)un.y * us;
+  const long long e1 = min((long long)xc, e0 + us);
   for (long long r0 = e0; r0 < e1; r0 += 128) {
     int cc[4];
 #pragma unroll
@@ -419,8 +432,9 @@ __device__ void reduce_unit(Env& E, Shared& sh, const QueueBufs& qb, int4 un, in
   const int v = un.x, chunk = un.y, ms = un.z, nch = un.w;
   const int L = g.len[v];
   const long long o = g.off[v];
-  const int s_lo = chunk * E.CH;
-  const int s_hi = min(L, s_lo + E.CH);
+  const int us = unit_span(L, nch);
+  const int s_lo = chunk * us;
+  const int s_hi = min(L, s_lo + us);
   const int limit = mode == M_DISTINCT ? kMaskBits : min(L, kMaskBits);
   const int nw = mask_words(L, mode);
   unsigned* sm = sh.mask[warp_id()];
@@ -652,7 +666,7 @@ __device__ void cta_push(Env& E, const QueueBufs& qb, QCount* qc) {
     const int u = i < cnt ? sh.cbuf[i] : -1;
     const int L = u >= 0 ? E.g.len[u] : 0;
     const bool isA = u >= 0 && L <= kSmall;
-    const int c = (u >= 0 && !isA) ? (L > CH ? (L + CH - 1) / CH : 1) : 0;
+    const int c = (u >= 0 && !isA) ? row_units(L, CH) : 0;
     if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
     int totA = 0, totU = 0;
     const int ea = block_excl_scan(isA ? 1 : 0, sh.sw, &totA);
@@ -747,8 +761,9 @@ __device__ __forceinline__ void claim4(Env& E, PushBuf& pb, const QueueBufs& nq,
 __device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi, long long xb, int xc,
                              const QueueBufs& nq, QCount* nc) {
   const HriBufs& H = E.hri;
-  const long long p0 = H.hoff[hi] + (long long)un.y * E.CH;
-  const long long p1 = min(H.hoff[hi + 1], p0 + E.CH);
+  const int us = unit_span(E.g.len[un.x], un.w);
+  const long long p0 = H.hoff[hi] + (long long)un.y * us;
+  const long long p1 = min(H.hoff[hi + 1], p0 + us);
   long long reads = 0;
   if (p0 < p1) {
     const int sf = (int)(H.pairs[p0] >> 32);
@@ -786,8 +801,8 @@ __device__ void expand_heavy(Env& E, PushBuf& pb, int4 un, const Rule& R, int hi
       }
     }
   }
-  const long long e0 = (long long)un.y * E.CH;
-  const long long e1 = min((long long)xc, e0 + E.CH);
+  const long long e0 = (long long)un.y * us;
+  const long long e1 = min((long long)xc, e0 + us);
   if (e0 < e1) {
     reads += e1 - e0;
     for (long long r0 = e0; r0 < e1; r0 += 128) {
@@ -878,8 +893,9 @@ __device__ void expand_unit(Env& E, PushBuf& pb, int4 un, const QueueBufs& nq, Q
   if (E.gskip && ld_cg(&E.gskip[E.gid[v]]) == 0) return;  // its graph has stopped
   const int L = g.len[v];
   const long long o = g.off[v];
-  const int s_lo = un.y * E.CH;
-  const int s_hi = min(L, s_lo + E.CH);
+  const int us = unit_span(L, un.w);
+  const int s_lo = un.y * us;
+  const int s_hi = min(L, s_lo + us);
   Rule R;
   R.v = v;
   R.cv = g.color[v] & kColorMask;
@@ -1199,7 +1215,8 @@ __device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const int
       }
     }
     if (u >= 0 && E.gskip && ld_cg(&E.gskip[E.gid[u]]) == 0) u = -1;  // its graph has stopped
-    const bool lng = u >= 0 && (g.len[u] > kPullLane || (E.hri_split && heavy_row(E, u) >= 0));
+    const bool lng = u >= 0 && (g.len[u] > kPullLane ||
+                                (E.hri_split && g.len[u] >= E.hri.min_live && heavy_row(E, u) >= 0));
     bool want = false;
     if (u >= 0 && !lng) want = pull_lane(E, inF, u, reads);
     push_ready(E, pb, nq, nc, u, want);
@@ -1537,15 +1554,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
           E.gskip = nullptr;
         }
       }
-      // Work units: the frontier's units were cut at the size recorded with
-      // its queue; the next frontier's are cut smaller when this one is
+      // Work units of the next frontier are cut smaller when this one is
       // small, so a small phase is not set by a few long units.
       {
-        const unsigned long long fch = ld_cg(&st->q[fs].ch);
-        E.CH = fch ? (int)fch : p.unit_slots;
         const long long items = (long long)ld_cg(&st->q[fs].countU) + ((long long)ld_cg(&st->q[fs].countA) + 31) / 32;
         E.CHp = unit_slots_for(items, nwarps, p.unit_slots);
-        if (leader) st->q[ns].ch = (unsigned long long)E.CHp;
       }
       // HB with a frontier of more than a sixteenth of the launch's vertices pulls
       const bool pull = V == DC_HB && (long long)(ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU)) * 16 >
@@ -1580,7 +1593,6 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         }
         E.gchg = V == DC_HB ? cur : nullptr;
       }
-      E.CH = E.CHp;  // the units E just pushed
       phase_reduce(E, sh, p.qb[nb], nc, ctr(), rmode, p.ncolor);
       ++ps;
       if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
@@ -1651,7 +1663,8 @@ __device__ void pred_unit(Env& E, int4 un, int* pred) {
   const int v = un.x;
   const int L = g.len[v];
   const long long o = g.off[v];
-  const int s_lo = un.y * E.CH, s_hi = min(L, s_lo + E.CH);
+  const int us = unit_span(L, un.w);
+  const int s_lo = un.y * us, s_hi = min(L, s_lo + us);
   const int pv = g.prop[v];
   int cnt = 0;
   for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
@@ -1697,7 +1710,8 @@ __device__ void release_unit(Env& E, PushBuf& pb, int4 un, int* pred, const Queu
   if (un.y == 0 && lane_id() == 0) cmax = max(cmax, commit_init(E, v));
   const int L = g.len[v];
   const long long o = g.off[v];
-  const int s_lo = un.y * E.CH, s_hi = min(L, s_lo + E.CH);
+  const int us = unit_span(L, un.w);
+  const int s_lo = un.y * us, s_hi = min(L, s_lo + us);
   const int pv = g.prop[v];
   for (int s0 = s_lo; s0 < s_hi; s0 += 32) {
     const int sidx = s0 + lane_id();

@@ -51,9 +51,9 @@ typedef struct {
                               pool grows up to this many slots (and shrinks back at the next
                               compaction that allows it); <= 0: 2 * pool_slots */
   int32_t grid_ctas;       /* CTAs of the persistent launches (dc_options.grid_ctas); 0: all */
-  int32_t heavy_min_live;  /* dc_options.heavy_min_live; a launch indexes only the rows of its own
-                              graphs, and only when its lines are at least 1/256 of their vertices;
-                              0: 2048, < 0: off */
+  int32_t heavy_min_live;  /* > 0: dc_options.heavy_min_live (a launch indexes only the rows of its
+                              own graphs, when its lines are at least 1/256 of their vertices);
+                              <= 0: off, every row is scanned */
   int32_t reserved[6];
 } dc_pool_options;
 
