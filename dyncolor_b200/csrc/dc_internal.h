@@ -38,9 +38,9 @@ enum { Q_LOOP0 = 0, Q_LOOP1 = 1, Q_LOOP2 = 2, Q_S1 = 3, Q_S2E = 4, Q_S2T = 5 };
 
 struct QCount {
   unsigned long long countA;  // class A items
-  unsigned long long countU;  // work units of single-unit rows, from the front of `units`
+  unsigned long long countU;  // work units (class B/C)
   unsigned long long masks;   // multi-unit mask words handed out
-  unsigned long long countH;  // work units of multi-unit rows, from the back of `units`
+  unsigned long long pad;
 };
 
 // Lives in device memory.  Fields up to `pool_used_start` persist across

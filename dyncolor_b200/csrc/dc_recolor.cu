@@ -54,7 +54,7 @@ struct Shared {
   int cbuf[kCtaBuf];                  // the CTA's newly marked vertices, pushed at the end of the phase
   int ccnt;                           // entries claimed in cbuf (may pass kCtaBuf)
   int sw[kWarps + 1];                 // block-scan scratch
-  unsigned long long qbase[3];        // queue positions the CTA's bulk push got (items, units, multi-unit rows' units)
+  unsigned long long qbase[2];        // queue positions the CTA's bulk push got (items, units)
 };
 
 __device__ __forceinline__ long long grab(unsigned long long* ctr) {
@@ -126,10 +126,7 @@ __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const
   }
   int c = 0;
   if (isU) c = row_units(L, CH);
-  // units of multi-unit rows fill the queue from the back, so a phase hands
-  // them out first and its long rows start at its beginning
-  const unsigned long long pn = warp_atomic_add(&qc->countU, c == 1 ? 1 : 0);
-  const unsigned long long ph = warp_atomic_add(&qc->countH, c > 1 ? c : 0);
+  const unsigned long long pu = warp_atomic_add(&qc->countU, c);
   if (isU) {
     int ms = -1;
     if (c > 1) {
@@ -144,27 +141,12 @@ __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const
       ms = (int)mo;
     }
     for (int q = 0; q < c; ++q) {
-      const long long k = c > 1 ? (long long)(ph + q) : (long long)pn;
-      if (k < qb.capU)
-        qb.units[c > 1 ? qb.capU - 1 - k : k] = make_int4(u, q, ms, c);
+      if ((long long)(pu + q) < qb.capU)
+        qb.units[pu + q] = make_int4(u, q, ms, c);
       else
         atomicOr(status, ST_OVERFLOW);
     }
   }
-}
-
-// The units of a queue: `nh` from the back (multi-unit rows), then the
-// rest from the front; unit i of the phase's index space.  Sets ST_OVERFLOW
-// when the two ends met.
-__device__ __forceinline__ long long queue_units(const QueueBufs& qb, const QCount* qc, long long* nh,
-                                                 unsigned* status) {
-  const long long h = (long long)ld_cg(&qc->countH), f = (long long)ld_cg(&qc->countU);
-  if (h + f > qb.capU && status) atomicOr(status, ST_OVERFLOW);
-  *nh = min(h, qb.capU);
-  return min(h + f, qb.capU);
-}
-__device__ __forceinline__ int4 unit_at(const QueueBufs& qb, long long nh, long long i) {
-  return i < nh ? qb.units[qb.capU - 1 - i] : qb.units[i - nh];
 }
 
 // Slots per work unit for a queue pushed while processing a phase of
@@ -598,15 +580,14 @@ __device__ void reduce_batchA(Env& E, Shared& sh, const QueueBufs& qb, long long
 __device__ void phase_reduce(Env& E, Shared& sh, const QueueBufs& qb, const QCount* qc,
                              unsigned long long* ctr, int mode, int* out) {
   const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
-  long long nh;
-  const long long cU = queue_units(qb, qc, &nh, &E.st->status);
+  const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
   const long long nAb = (cA + 31) / 32;
   const long long total = cU + nAb;
   Grabber gb(ctr, total, E.nwarps);
   long long i;
   while (gb.next(i)) {
     if (i < cU)
-      reduce_unit(E, sh, qb, unit_at(qb, nh, i), mode, out);
+      reduce_unit(E, sh, qb, qb.units[i], mode, out);
     else
       reduce_batchA(E, sh, qb, cA, i - cU, mode, out);
   }
@@ -687,13 +668,11 @@ __device__ void cta_push(Env& E, const QueueBufs& qb, QCount* qc) {
     const bool isA = u >= 0 && L <= kSmall;
     const int c = (u >= 0 && !isA) ? row_units(L, CH) : 0;
     if (E.gpush && u >= 0) atomicAdd(&E.gpush[E.gid[u]], 1);
-    int totA = 0, totU = 0, totH = 0;
+    int totA = 0, totU = 0;
     const int ea = block_excl_scan(isA ? 1 : 0, sh.sw, &totA);
-    const int eu = block_excl_scan(c == 1 ? 1 : 0, sh.sw, &totU);
-    const int eh = block_excl_scan(c > 1 ? c : 0, sh.sw, &totH);
+    const int eu = block_excl_scan(c, sh.sw, &totU);
     if (threadIdx.x == 0 && totA) sh.qbase[0] = atomicAdd(&qc->countA, (unsigned long long)totA);
     if (threadIdx.x == 32 && totU) sh.qbase[1] = atomicAdd(&qc->countU, (unsigned long long)totU);
-    if (threadIdx.x == 64 && totH) sh.qbase[2] = atomicAdd(&qc->countH, (unsigned long long)totH);
     __syncthreads();
     if (isA) {
       const unsigned long long pa = sh.qbase[0] + ea;
@@ -717,10 +696,10 @@ __device__ void cta_push(Env& E, const QueueBufs& qb, QCount* qc) {
           ms = (int)mo;
         }
       }
+      const unsigned long long pu = sh.qbase[1] + eu;
       for (int q = 0; ok && q < c; ++q) {
-        const long long k = c > 1 ? (long long)(sh.qbase[2] + eh + q) : (long long)(sh.qbase[1] + eu);
-        if (k < qb.capU)
-          qb.units[c > 1 ? qb.capU - 1 - k : k] = make_int4(u, q, ms, c);
+        if ((long long)(pu + q) < qb.capU)
+          qb.units[pu + q] = make_int4(u, q, ms, c);
         else
           atomicOr(&E.st->status, ST_OVERFLOW);
       }
@@ -1043,8 +1022,7 @@ __device__ void expand_batchA(Env& E, PushBuf& pb, const QueueBufs& fq, long lon
 __device__ void phase_expand(Env& E, Shared& sh, const QueueBufs& fq, const QCount* fc,
                              const QueueBufs& nq, QCount* nc, unsigned long long* ctr) {
   const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
-  long long nh;
-  const long long cU = queue_units(fq, fc, &nh, &E.st->status);
+  const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
   const long long nAb = (cA + 31) / 32;
   const long long total = cU + nAb;
   PushBuf pb;
@@ -1054,7 +1032,7 @@ __device__ void phase_expand(Env& E, Shared& sh, const QueueBufs& fq, const QCou
   long long i;
   while (gb.next(i)) {
     if (i < cU)
-      expand_unit(E, pb, unit_at(fq, nh, i), nq, nc);
+      expand_unit(E, pb, fq.units[i], nq, nc);
     else
       expand_batchA(E, pb, fq, cA, i - cU, nq, nc);
   }
@@ -1075,11 +1053,10 @@ enum Commit {
 };
 
 // Item i of a queue: class A items first, then units with chunk 0.
-__device__ __forceinline__ int queue_item(const QueueBufs& qb, long long cA, long long nh, long long total,
-                                          long long i) {
+__device__ __forceinline__ int queue_item(const QueueBufs& qb, long long cA, long long total, long long i) {
   if (i < cA) return qb.itemsA[i];
   if (i < total) {
-    const int4 un = unit_at(qb, nh, i - cA);
+    const int4 un = qb.units[i - cA];
     if (un.y == 0) return un.x;
   }
   return -1;
@@ -1109,12 +1086,11 @@ constexpr int kPullLane = 64;  // rows up to this length are walked by one lane
 __device__ void phase_mark_frontier(Env& E, const QueueBufs& fq, const QCount* fc, unsigned* inF,
                                     long long gwarp, long long nwarps) {
   const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
-  long long nh;
-  const long long cU = queue_units(fq, fc, &nh, nullptr);
+  const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
   const long long total = cA + cU;
   long long cov = 0;
   for (long long i0 = gwarp * 32; i0 < total; i0 += nwarps * 32) {
-    const int v = queue_item(fq, cA, nh, total, i0 + lane_id());
+    const int v = queue_item(fq, cA, total, i0 + lane_id());
     if (v < 0) continue;
     if (E.gskip && ld_cg(&E.gskip[E.gid[v]]) == 0) continue;  // its graph has stopped
     atomicOr(&inF[v >> 5], 1u << (v & 31));
@@ -1266,14 +1242,13 @@ __device__ void phase_commit(Env& E, const QueueBufs& qb, const QCount* qc, int 
                              unsigned long long* items_stat, int* chg_flag) {
   const GraphDev& g = E.g;
   const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
-  long long nh;
-  const long long cU = queue_units(qb, qc, &nh, nullptr);
+  const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
   const long long total = cA + cU;
   long long items = 0;
   int cmax_local = -1;
   bool changed = false;
   for (long long i0 = gwarp * 32; i0 < total; i0 += nwarps * 32) {
-    const int v = queue_item(qb, cA, nh, total, i0 + lane_id());
+    const int v = queue_item(qb, cA, total, i0 + lane_id());
     int push = -1;
     int first = -1;  // first colour change since the heavy-row index was built
     int first_c0 = 0;  // its colour until then
@@ -1541,7 +1516,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
     const QCount* f0c = &st->q[Q_LOOP0];
     long long it = 0;
     const int rmode = V == DC_HI ? M_MEX_ALL : M_MEX_PRIOR;
-    bool go = (ld_cg(&f0c->countA) + ld_cg(&f0c->countU) + ld_cg(&f0c->countH)) > 0;
+    bool go = (ld_cg(&f0c->countA) + ld_cg(&f0c->countU)) > 0;
     while (go) {
       if (it >= p.iter_cap) {
         if (leader) atomicOr(&st->status, ST_ITER);
@@ -1555,7 +1530,6 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
         QCount* z = &st->q[(fs + 2) % 3];
         z->countA = 0;
         z->countU = 0;
-        z->countH = 0;
         z->masks = 0;
         st->a_count = 0;  // every warp read it before the append phase's barrier
       }
@@ -1583,14 +1557,11 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       // Work units of the next frontier are cut smaller when this one is
       // small, so a small phase is not set by a few long units.
       {
-        const long long items = (long long)(ld_cg(&st->q[fs].countU) + ld_cg(&st->q[fs].countH)) +
-                                ((long long)ld_cg(&st->q[fs].countA) + 31) / 32;
+        const long long items = (long long)ld_cg(&st->q[fs].countU) + ((long long)ld_cg(&st->q[fs].countA) + 31) / 32;
         E.CHp = unit_slots_for(items, nwarps, p.unit_slots);
       }
       // HB with a frontier of more than a sixteenth of the launch's vertices pulls
-      const bool pull = V == DC_HB &&
-                        (long long)(ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU) + ld_cg(&st->q[fs].countH)) *
-                                16 >
+      const bool pull = V == DC_HB && (long long)(ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU)) * 16 >
                                           (p.ranges ? (long long)p.ranges[1] : (long long)g.n);
       E.cta_stage = true;
       if (pull) {
@@ -1605,7 +1576,7 @@ __global__ void __launch_bounds__(kThreads, 2) recolor_kernel(RecolorParams p) {
       if (!grid_sync(st, bar, p.bar_timeout_ns)) return;
       lap(1);
       const QCount* nc = &st->q[ns];
-      const long long nq = (long long)(ld_cg(&nc->countA) + ld_cg(&nc->countU) + ld_cg(&nc->countH));
+      const long long nq = (long long)(ld_cg(&nc->countA) + ld_cg(&nc->countU));
       if (V == DC_HI && nq == 0) break;
       // R
       if (leader) st->chg[(it + 1) & 1] = 0;
@@ -1828,14 +1799,13 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
     const QueueBufs& qb = p.qb[2];
     const QCount* qc = &st->q[Q_S1];
     const long long cA = min((long long)ld_cg(&qc->countA), qb.capA);
-    long long nh;
-    const long long cU = queue_units(qb, qc, &nh, &st->status);
+    const long long cU = min((long long)ld_cg(&qc->countU), qb.capU);
     const long long total = cU + (cA + 31) / 32;
     Grabber gb(ctr(), total, E.nwarps);
     long long i;
     while (gb.next(i)) {
       if (i < cU)
-        pred_unit(E, unit_at(qb, nh, i), pred);
+        pred_unit(E, qb.units[i], pred);
       else
         pred_batchA(E, qb, cA, i - cU, pred);
     }
@@ -1852,7 +1822,7 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
   int fs = Q_LOOP0, fb = 0;
   long long it = 0;
   int cmax = -1;
-  while (ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU) + ld_cg(&st->q[fs].countH) > 0) {
+  while (ld_cg(&st->q[fs].countA) + ld_cg(&st->q[fs].countU) > 0) {
     if (it >= p.iter_cap) {
       if (leader) atomicOr(&st->status, ST_ITER);
       break;
@@ -1864,7 +1834,6 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
       QCount* z = &st->q[(fs + 2) % 3];
       z->countA = 0;
       z->countU = 0;
-      z->countH = 0;
       z->masks = 0;
     }
     // R: the mex over the neighbours before each frontier vertex
@@ -1876,8 +1845,7 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
       const QueueBufs& fq = p.qb[fb];
       const QCount* fc = &st->q[fs];
       const long long cA = min((long long)ld_cg(&fc->countA), fq.capA);
-      long long nh;
-      const long long cU = queue_units(fq, fc, &nh, &st->status);
+      const long long cU = min((long long)ld_cg(&fc->countU), fq.capU);
       const long long total = cU + (cA + 31) / 32;
       PushBuf pb;
       pb.buf = sh.pbuf[warp_id()];
@@ -1886,7 +1854,7 @@ __global__ void __launch_bounds__(kThreads, 2) init_color_kernel(RecolorParams p
       long long i;
       while (gb.next(i)) {
         if (i < cU)
-          release_unit(E, pb, unit_at(fq, nh, i), pred, p.qb[nb], &st->q[ns], cmax);
+          release_unit(E, pb, fq.units[i], pred, p.qb[nb], &st->q[ns], cmax);
         else
           release_batchA(E, pb, fq, cA, i - cU, pred, p.qb[nb], &st->q[ns], cmax);
       }
