@@ -29,7 +29,7 @@ constexpr int kTomb = -1;           // tombstoned adjacency slot
 constexpr unsigned kMarkBit = 1u << 30;
 constexpr int kColorMask = (1 << 30) - 1;
 constexpr int kNumQueues = 6;       // logical queue counter slots
-constexpr int kUnitSlotsDefault = 2048;  // adjacency slots per warp work unit
+constexpr int kUnitSlotsDefault = 4096;  // adjacency slots per warp work unit
 constexpr long long kLoadPiece = 1ll << 27;  // edge pairs per structural launch of a graph load
 constexpr int kBarrierTimeoutMsDefault = 20000;  // grid-barrier wait limit unless the options set one
 

@@ -1145,51 +1145,69 @@ __device__ __forceinline__ bool pull_lane(const Env& E, const unsigned* inF, int
   return false;
 }
 
-// The same for a long row, by the whole warp (all lanes call; u uniform).
-__device__ bool pull_warp(const Env& E, const unsigned* inF, int u, long long& reads) {
+// Long rows four at a time: lane group g (8 lanes) walks row rows[g], 8
+// entries per step, until a hit or the row's end; the warp loops while any
+// group is still walking.  All lanes call; returns this group's verdict.
+__device__ bool pull_group(const Env& E, const unsigned* inF, int x, long long& reads) {
   const GraphDev& g = E.g;
-  const int pu = g.prop[u];
-  const bool fu = in_bits(inF, u);
-  const int cu = (int)((unsigned)E.cp[u] & (unsigned)kColorMask);
-  const int hi = E.hri_split ? heavy_row(E, u) : -1;
-  if (hi >= 0) {
-    // prior neighbours first: only they can mark u
-    const long long pb = E.hri.hoff[hi];
-    const int nh = E.hri.hsplit[hi];
-    for (int s0 = 0; s0 < nh; s0 += 32) {
-      const int s = s0 + lane_id();
-      bool hit = false;
-      if (s < nh) {
-        const int w = (int)(unsigned)E.hri.pairs[pb + s];
-        hit = in_bits(inF, w) ||
-              (fu && (int)((unsigned)E.cp[w] & (unsigned)kColorMask) == cu);
-      }
-      reads += min(32, nh - s0);
-      if (__any_sync(0xffffffffu, hit)) return true;
+  const int grp = lane_id() >> 3, sub = lane_id() & 7;
+  const unsigned gmask = 0xffu << (grp * 8);
+  int lim = 0, pu = 0, cu = 0;
+  long long base = 0;
+  bool fu = false, idx = false;
+  if (x >= 0) {
+    pu = g.prop[x];
+    fu = in_bits(inF, x);
+    cu = (int)((unsigned)E.cp[x] & (unsigned)kColorMask);
+    const int hi = E.hri_split ? heavy_row(E, x) : -1;
+    if (hi >= 0) {
+      idx = true;
+      base = E.hri.hoff[hi];
+      lim = E.hri.hsplit[hi];
+    } else {
+      base = g.off[x];
+      lim = g.len[x];
     }
-    return false;
   }
-  const int L = g.len[u];
-  const long long o = g.off[u];
-  for (int s0 = 0; s0 < L; s0 += 32) {
-    const int s = s0 + lane_id();
+  bool done = x < 0, m = false;
+  for (int s0 = 0;; s0 += 8) {
+    const bool act = !done && s0 < lim;
+    if (!__any_sync(0xffffffffu, act)) break;
     bool hit = false;
-    const int w = s < L ? g.adj[o + s] : -1;
-    if (w >= 0) {
-      const unsigned long long x = E.cp[w];
-      hit = is_prior((int)(x >> 32), w, pu, u) &&
-            (in_bits(inF, w) || (fu && (int)((unsigned)x & (unsigned)kColorMask) == cu));
+    if (act) {
+      const int s = s0 + sub;
+      if (s < lim) {
+        ++reads;
+        if (idx) {
+          const int w = (int)(unsigned)E.hri.pairs[base + s];
+          hit = in_bits(inF, w) || (fu && (int)((unsigned)E.cp[w] & (unsigned)kColorMask) == cu);
+        } else {
+          const int w = g.adj[base + s];
+          if (w >= 0) {
+            const unsigned long long xx = E.cp[w];
+            hit = is_prior((int)(xx >> 32), w, pu, x) &&
+                  (in_bits(inF, w) || (fu && (int)((unsigned)xx & (unsigned)kColorMask) == cu));
+          }
+        }
+      }
     }
-    reads += min(32, L - s0);
-    if (__any_sync(0xffffffffu, hit)) return true;
+    const unsigned bal = __ballot_sync(0xffffffffu, hit) & gmask;
+    if (act) {
+      if (bal) {
+        m = true;
+        done = true;
+      } else if (s0 + 8 >= lim) {
+        done = true;
+      }
+    }
   }
-  return false;
+  return m;
 }
 
 // Every vertex of the launch's graphs (all vertices, or the vertex ranges
 // of a pool launch) decides whether it joins the next frontier; lanes take
 // rows of up to kPullLane slots, the warp then takes the longer rows of its
-// 32 vertices one by one.
+// 32 vertices four at a time (8 lanes each).
 __device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const int* ranges, const QueueBufs& nq,
                               QCount* nc, long long gwarp, long long nwarps) {
   const GraphDev& g = E.g;
@@ -1222,13 +1240,20 @@ __device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const int
     push_ready(E, pb, nq, nc, u, want);
     unsigned todo = __ballot_sync(0xffffffffu, lng);
     while (todo) {
-      const int l = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const int v = __shfl_sync(0xffffffffu, u, l);
-      long long r = 0;
-      const bool m = pull_warp(E, inF, v, r);
-      if (lane_id() == 0) reads += r;
-      push_ready(E, pb, nq, nc, v, m && lane_id() == 0);
+      int rows[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        rows[k] = -1;
+        if (todo) {
+          const int l = __ffs(todo) - 1;
+          todo &= todo - 1;
+          rows[k] = __shfl_sync(0xffffffffu, u, l);
+        }
+      }
+      const int grp = lane_id() >> 3;
+      const int x = grp == 0 ? rows[0] : grp == 1 ? rows[1] : grp == 2 ? rows[2] : rows[3];
+      const bool m = pull_group(E, inF, x, reads);
+      push_ready(E, pb, nq, nc, x, m && (lane_id() & 7) == 0);
     }
   }
   if (pb.cnt > 0) flush(E, pb, nq, nc, pb.cnt);

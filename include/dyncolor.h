@@ -75,7 +75,7 @@ typedef struct {
   float slack;           /* row capacity = live * slack when a row is (re)allocated; <= 1: 1.25 */
   int32_t blocks_per_sm; /* persistent-kernel CTAs per SM; 0: from occupancy */
   int64_t reserve_slots; /* initial adjacency pool size hint in slots; 0: automatic */
-  int32_t unit_slots;    /* adjacency slots per warp work unit (multiple of 128); 0: 2048 */
+  int32_t unit_slots;    /* adjacency slots per warp work unit (multiple of 128); 0: 4096 */
   int32_t cuda_graph;    /* 1: replay each batch's launches from a captured CUDA graph */
   int32_t heavy_min_live; /* rows with at least this many live slots get a per-batch index (HI: by
                              colour, HB: by priority) used by batches of at least n/256 lines;

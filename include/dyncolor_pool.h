@@ -44,7 +44,7 @@ typedef struct {
   int64_t iter_cap;        /* recolour-loop iteration cap; <= 0: 1<<20 */
   float slack;             /* row capacity = live * slack when a row is (re)allocated; <= 1: 1.25 */
   int32_t blocks_per_sm;   /* persistent-kernel CTAs per SM; 0: from occupancy */
-  int32_t unit_slots;      /* adjacency slots per warp work unit; 0: 2048 */
+  int32_t unit_slots;      /* adjacency slots per warp work unit; 0: 4096 */
   int32_t cuda_graph;      /* 1: replay each launch from a captured CUDA graph */
   int64_t stage_slots;     /* device staging for spill and reload (4-byte slots); <= 0: 2^25 */
   int64_t pool_slots_max;  /* hard limit: when the graphs of one launch alone outgrow pool_slots, the
