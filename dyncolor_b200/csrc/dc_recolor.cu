@@ -1079,7 +1079,7 @@ __device__ __forceinline__ void push_ready(Env& E, PushBuf& pb, const QueueBufs&
 // is in the frontier and a neighbour prior to u has u's colour -- the same
 // set the rule marks from the frontier side (HB/gpuFunctions_undir.cuh:
 // 259-291).  Frontier membership is a bitmap built from the queue first.
-constexpr int kPullLane = 64;  // rows up to this length are walked by one lane
+constexpr int kPullLane = 256;  // rows up to this length are walked by one lane
 
 // Sets the membership bit of every frontier vertex and counts the entries
 // the rule covers (the frontier rows' live entries).
