@@ -317,7 +317,7 @@ def hbm_peak():
 # launch, from ncu captures (dram__bytes_read.sum + dram__bytes_write.sum,
 # one pass) of this bench's workloads; keyed by (variant, scale, edge factor,
 # lines).  The summary that each figure comes from is in profiles/.
-MEASURED_DRAM_BYTES_PER_ENTRY = {("hi", 24, 16, 1_000_000): 1.333, ("hi", 22, 16, 250_000): 1.170}
+MEASURED_DRAM_BYTES_PER_ENTRY = {("hi", 24, 16, 1_000_000): 1.285, ("hi", 22, 16, 250_000): 1.127}
 
 
 def load_traffic(variant: str, scale: int, ef: int, lines: int):
