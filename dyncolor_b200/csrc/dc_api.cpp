@@ -597,7 +597,7 @@ dc_status dc_options_default(dc_options* opt) {
   opt->blocks_per_sm = 0;
   opt->reserve_slots = 0;
   opt->unit_slots = kUnitSlotsDefault;
-  opt->heavy_min_live = kHeavyMinLive;
+  opt->heavy_min_live = 0;  // per variant: dc_create picks it
   opt->barrier_timeout_ms = kBarrierTimeoutMsDefault;
   return DC_OK;
 }
@@ -615,7 +615,7 @@ dc_status dc_create(dc_ctx** out, const dc_options* opt) {
   if (!(o.slack > 1.0f)) o.slack = 1.25f;
   if (o.unit_slots <= 0) o.unit_slots = kUnitSlotsDefault;
   if (o.unit_slots % 128 != 0 || o.unit_slots < 128) return DC_E_INVAL;
-  if (o.heavy_min_live == 0) o.heavy_min_live = kHeavyMinLive;
+  if (o.heavy_min_live == 0) o.heavy_min_live = o.variant == DC_HB ? kHeavyMinLiveHB : kHeavyMinLive;
   if (o.heavy_min_live < 0) o.heavy_min_live = 0;  // off
   if (o.heavy_min_live > 0 && o.heavy_min_live < 64) o.heavy_min_live = 64;
   if (o.barrier_timeout_ms <= 0) o.barrier_timeout_ms = kBarrierTimeoutMsDefault;

@@ -154,7 +154,8 @@ struct StructParams {
 // for such a row it reads the head of the ordered copy, the segment of
 // colour color[v], and the list, instead of gathering every neighbour's
 // colour.
-constexpr int kHeavyMinLive = 2048;
+constexpr int kHeavyMinLive = 2048;   // HI
+constexpr int kHeavyMinLiveHB = 256;  // HB: its index only splits rows by priority, cheap to build
 // A batch uses the index when lines * kIndexBatchRatio >= n.
 constexpr long long kIndexBatchRatio = 256;
 constexpr int kHriBins = 1024;  // exact colour order below 1023; colours >= 1023 share the first bin

@@ -79,7 +79,8 @@ typedef struct {
   int32_t cuda_graph;    /* 1: replay each batch's launches from a captured CUDA graph */
   int32_t heavy_min_live; /* rows with at least this many live slots get a per-batch index (HI: by
                              colour, HB: by priority) used by batches of at least n/256 lines;
-                             0: 2048, < 0: off.  Results are the same either way. */
+                             0: 2048 for HI, 256 for HB; < 0: off.  Results are the same either
+                             way. */
   int32_t barrier_timeout_ms; /* limit of every device-side grid-barrier wait; 0: 20,000 ms.  A wait
                                  that runs out ends the launch with DC_E_TIMEOUT instead of hanging,
                                  and the context then refuses further work (DC_E_STATE). */
