@@ -1125,6 +1125,24 @@ __device__ __forceinline__ bool pull_lane(const Env& E, const unsigned* inF, int
   const int pu = g.prop[u];
   const bool fu = in_bits(inF, u);
   const int cu = (int)((unsigned)E.cp[u] & (unsigned)kColorMask);
+  const int hi = (E.hri_split && L >= E.hri.min_live) ? heavy_row(E, u) : -1;
+  if (hi >= 0) {
+    // an indexed row lists its prior neighbours first: only they can mark u
+    const long long pb = E.hri.hoff[hi];
+    const int nh = E.hri.hsplit[hi];
+    for (int s0 = 0; s0 < nh; s0 += 4) {
+      int w[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) w[j] = s0 + j < nh ? (int)(unsigned)E.hri.pairs[pb + s0 + j] : -1;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) reads += w[j] >= 0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (w[j] >= 0 && (in_bits(inF, w[j]) || (fu && (int)((unsigned)E.cp[w[j]] & (unsigned)kColorMask) == cu)))
+          return true;
+    }
+    return false;
+  }
   for (int s0 = 0; s0 < L; s0 += 4) {
     int w[4];
     unsigned long long x[4];
@@ -1233,8 +1251,7 @@ __device__ void phase_pull_hb(Env& E, Shared& sh, const unsigned* inF, const int
       }
     }
     if (u >= 0 && E.gskip && ld_cg(&E.gskip[E.gid[u]]) == 0) u = -1;  // its graph has stopped
-    const bool lng = u >= 0 && (g.len[u] > kPullLane ||
-                                (E.hri_split && g.len[u] >= E.hri.min_live && heavy_row(E, u) >= 0));
+    const bool lng = u >= 0 && g.len[u] > kPullLane;
     bool want = false;
     if (u >= 0 && !lng) want = pull_lane(E, inF, u, reads);
     push_ready(E, pb, nq, nc, u, want);
