@@ -151,14 +151,14 @@ __device__ __forceinline__ void warp_push(const QueueBufs& qb, QCount* qc, const
 
 // Slots per work unit for a queue pushed while processing a phase of
 // `items` work items with `nwarps` warps: the configured size while the
-// phase keeps every warp busy, a quarter or an eighth of it (at least 128,
-// a multiple of 128) when it does not.
+// phase keeps every warp busy, a half or a quarter of it (at least 128, a
+// multiple of 128) when it does not.
 __device__ __forceinline__ int unit_slots_for(long long items, long long nwarps, int ch) {
   int d = 1;
   if (items < nwarps / 2)
-    d = 8;
-  else if (items < 2 * nwarps)
     d = 4;
+  else if (items < 2 * nwarps)
+    d = 2;
   const int c = (ch / d) & ~127;
   return c < 128 ? 128 : c;
 }
