@@ -77,7 +77,10 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     HriBufs& h = ctx->hri;
     h.min_live = ctx->opt.heavy_min_live;
     h.cap_rows = std::min<long long>(n + 1, ctx->pool_cap / h.min_live + 1);
-    h.cap_pairs = ctx->pool_cap / 4 + 4096;  // R-MAT scale 24: rows >= 2048 hold 236 M of 1.57 G slots
+    // R-MAT scale 24 (1.57 G pool slots): rows >= 2048 hold 236 M slots, rows
+    // >= 256 339 M, rows >= 128 414 M.  HB's 4-byte ids get twice the entries
+    // in the same bytes.
+    h.cap_pairs = hi ? ctx->pool_cap / 4 + 4096 : ctx->pool_cap / 2 + 8192;
     h.cap_exc = hi ? h.cap_pairs : 1;       // a row's change list holds at most its live neighbours
     h.cap_a = hi ? n / 8 + ctx->pool_cap / 512 + 1024 : 1;  // items of 512 slots
     h.cap_hist = hi ? std::min<long long>(h.cap_rows, 1ll << 16) : 0;
@@ -86,11 +89,13 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     if ((s = dalloc(ctx, &h.xoff, h.cap_rows + 1, "change-list offsets")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.xcnt, h.cap_rows, "change-list counts")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.hsplit, h.cap_rows, "priority splits")) != DC_OK) return s;
-    if ((s = dalloc(ctx, &h.pairs, h.cap_pairs, "ordered neighbours")) != DC_OK) return s;
     if (hi) {
+      if ((s = dalloc(ctx, &h.pairs, h.cap_pairs, "ordered neighbours")) != DC_OK) return s;
       if ((s = dalloc(ctx, &h.xv, h.cap_exc, "change lists")) != DC_OK) return s;
       if ((s = dalloc(ctx, &h.alist, h.cap_a, "append queue")) != DC_OK) return s;
       if ((s = dalloc(ctx, &h.hist, h.cap_hist * kHriBins, "heavy-row colour counts")) != DC_OK) return s;
+    } else {
+      if ((s = dalloc(ctx, &h.ids, h.cap_pairs, "split neighbours")) != DC_OK) return s;
     }
   }
   if (!ctx->bmA) {
@@ -691,6 +696,7 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->hri.xoff);
   dfree(ctx, &ctx->hri.xcnt);
   dfree(ctx, &ctx->hri.pairs);
+  dfree(ctx, &ctx->hri.ids);
   dfree(ctx, &ctx->hri.xv);
   dfree(ctx, &ctx->hri.alist);
   dfree(ctx, &ctx->hri.hist);

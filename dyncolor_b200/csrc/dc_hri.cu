@@ -12,7 +12,7 @@
 //             bin), written as (colour << 32) | neighbour; the first
 //             cap_hist rows also keep their per-colour counts
 //   split (HB) one CTA per row: the neighbours prior to the row's vertex in
-//             LDF order first, then the rest
+//             LDF order first, then the rest, as 4-byte ids
 #include "dc_device.cuh"
 
 namespace dc {
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kHriThreads) hri_split_kernel(GraphDev g, HriB
       if (u < 0) continue;
       const int pos = atomicAdd(&s_cur[is_prior(g.prop[u], u, pv, v) ? 0 : 1], 1);
       if (pos < room)
-        h.pairs[base + pos] = (unsigned)u;
+        h.ids[base + pos] = u;
       else
         atomicOr(&st->status, ST_OVERFLOW);
     }

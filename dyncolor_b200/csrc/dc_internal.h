@@ -163,16 +163,17 @@ struct HriBufs {
   int* hid;                   // n: index of v's ordered copy, or -1
   int* hrow;                  // cap_rows: vertex of index i
   long long* hoff;            // cap_rows + 1: start of row i in pairs
-  unsigned long long* pairs;  // cap_pairs: (colour << 32) | neighbour
-  long long* xoff;            // cap_rows + 1: start of row i's change list
+  unsigned long long* pairs;  // HI, cap_pairs: (colour << 32) | neighbour
+  int* ids;                   // HB, cap_pairs: neighbour ids (see hsplit)
+  long long* xoff;           // cap_rows + 1: start of row i's change list
   int* xcnt;                  // cap_rows: entries appended to row i's change list (> capacity: overflow)
   int* xv;                    // cap_exc: changed neighbours
   unsigned* bmF;              // n/32 + 1: colour changed since the index was built
   int2* alist;                // cap_a: (vertex, chunk) of first changes, for the append phase
   int* hist;                  // cap_hist * kHriBins: row i's count of neighbours per launch-start colour
                               // that have not changed colour since (the append phase takes them off)
-  int* hsplit;                // HB, cap_rows: row i's copy holds its prior neighbours first, hsplit[i]
-                              // of them, then the rest
+  int* hsplit;                // HB, cap_rows: row i's copy (in ids) holds its prior neighbours first,
+                              // hsplit[i] of them, then the rest
   long long cap_rows, cap_pairs, cap_exc, cap_a, cap_hist;
   int min_live;               // 0: no index
   // Vertex ranges the index covers (nullptr: every vertex): [count, total,

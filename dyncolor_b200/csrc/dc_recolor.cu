@@ -401,7 +401,7 @@ __device__ bool reduce_split(Env& E, Shared& sh, int4 un, int* out) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int idx = r0 + j * 32 + lane_id();
-      cc[j] = idx < nh ? (int)((unsigned)E.cp[(int)(unsigned)H.pairs[pb + idx]] & (unsigned)kColorMask) : -1;
+      cc[j] = idx < nh ? (E.g.color[H.ids[pb + idx]] & kColorMask) : -1;
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -1133,12 +1133,12 @@ __device__ __forceinline__ bool pull_lane(const Env& E, const unsigned* inF, int
     for (int s0 = 0; s0 < nh; s0 += 4) {
       int w[4];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) w[j] = s0 + j < nh ? (int)(unsigned)E.hri.pairs[pb + s0 + j] : -1;
+      for (int j = 0; j < 4; ++j) w[j] = s0 + j < nh ? E.hri.ids[pb + s0 + j] : -1;
 #pragma unroll
       for (int j = 0; j < 4; ++j) reads += w[j] >= 0;
 #pragma unroll
       for (int j = 0; j < 4; ++j)
-        if (w[j] >= 0 && (in_bits(inF, w[j]) || (fu && (int)((unsigned)E.cp[w[j]] & (unsigned)kColorMask) == cu)))
+        if (w[j] >= 0 && (in_bits(inF, w[j]) || (fu && (g.color[w[j]] & kColorMask) == cu)))
           return true;
     }
     return false;
@@ -1197,8 +1197,8 @@ __device__ bool pull_group(const Env& E, const unsigned* inF, int x, long long& 
       if (s < lim) {
         ++reads;
         if (idx) {
-          const int w = (int)(unsigned)E.hri.pairs[base + s];
-          hit = in_bits(inF, w) || (fu && (int)((unsigned)E.cp[w] & (unsigned)kColorMask) == cu);
+          const int w = E.hri.ids[base + s];
+          hit = in_bits(inF, w) || (fu && (g.color[w] & kColorMask) == cu);
         } else {
           const int w = g.adj[base + s];
           if (w >= 0) {
