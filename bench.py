@@ -638,9 +638,9 @@ def run_ours(args, dist: Dist):
         "config": config(args, w),
         "e2e": {"value": total_updates / e2e_s if e2e_s > 0 else None, "unit": UNIT,
                 "h2d_bytes_per_step": 12 * k, "d2h_bytes_per_step": 4 * int(w["n"])},
-        # per batch: structural + recolour launches, and the three heavy-row
+        # per batch: structural + recolour launches, and the four heavy-row
         # index kernels when the batch uses the index (lines * 256 >= n)
-        "gpu_launches": (5 if args.heavy_min_live >= 0 and k * 256 >= int(w["n"]) else 2) * K,
+        "gpu_launches": (6 if args.heavy_min_live >= 0 and k * 256 >= int(w["n"]) else 2) * K,
         "roofline": roof,
         "clocks": clk,
         "detail": {

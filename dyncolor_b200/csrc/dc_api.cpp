@@ -89,6 +89,7 @@ dc_status ensure_recolor_scratch(dc_ctx* ctx) {
     if ((s = dalloc(ctx, &h.xoff, h.cap_rows + 1, "change-list offsets")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.xcnt, h.cap_rows, "change-list counts")) != DC_OK) return s;
     if ((s = dalloc(ctx, &h.hsplit, h.cap_rows, "priority splits")) != DC_OK) return s;
+    if ((s = dalloc(ctx, &h.bcnt, 64, "row length classes")) != DC_OK) return s;
     if (hi) {
       if ((s = dalloc(ctx, &h.pairs, h.cap_pairs, "ordered neighbours")) != DC_OK) return s;
       if ((s = dalloc(ctx, &h.xv, h.cap_exc, "change lists")) != DC_OK) return s;
@@ -701,6 +702,7 @@ void dc_destroy(dc_ctx* ctx) {
   dfree(ctx, &ctx->hri.alist);
   dfree(ctx, &ctx->hri.hist);
   dfree(ctx, &ctx->hri.hsplit);
+  dfree(ctx, &ctx->hri.bcnt);
   dfree(ctx, &ctx->d_ranges);
   dfree(ctx, &ctx->off);
   dfree(ctx, &ctx->len);

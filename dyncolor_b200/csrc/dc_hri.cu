@@ -1,12 +1,15 @@
 // dc_hri.cu -- heavy-row index of the recolouring loop, rebuilt before
 // every recolour launch (after the structural update of the batch).
 //
-//   classify  rows with at least min_live live slots get an index i (in
-//             arrival order; the order never affects results) and clear the
-//             changed-colour bitmap
+//   count     rows with at least min_live live slots, per length class
+//             floor(log2(live))
+//   classify  those rows get an index i, longest class first (arrival
+//             order within a class; the order never affects results), and
+//             the changed-colour bitmap is cleared
 //   offsets   one CTA: exclusive scans of the rows' live counts (ordered
 //             copies) and of their change-list capacities; rows past the
-//             buffers' capacity lose their index and are scanned in full
+//             buffers' capacity (the shortest) lose their index and are
+//             scanned in full
 //   fill (HI) one CTA per row: counting sort of the row's live neighbours
 //             by colour, descending (colours >= kHriBins - 1 share the first
 //             bin), written as (colour << 32) | neighbour; the first
@@ -27,30 +30,19 @@ __device__ __forceinline__ int hri_bin(int c) { return c < kHriBins - 1 ? c : kH
 // list once per launch (at its first colour change), so it never overflows.
 __device__ __forceinline__ long long xcap(int live) { return live; }
 
-__device__ __forceinline__ void classify_one(const GraphDev& g, const HriBufs& h, DevState* st, int v) {
-  int id = -1;
-  if (g.live[v] >= h.min_live) {
-    const unsigned long long i = atomicAdd(&st->hcount, 1ull);
-    if ((long long)i < h.cap_rows) {
-      id = (int)i;
-      h.hrow[i] = v;
-    }
-  }
-  h.hid[v] = id;
-}
+// Length class of a row with live >= 1 slots: floor(log2(live)).
+__device__ __forceinline__ int len_class(int live) { return 31 - __clz(live); }
 
-__global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
+// Calls f(v) for every vertex the index covers: all of them, or those of
+// h.ranges (one index space over the ranges, binary search for the range).
+template <typename F>
+__device__ __forceinline__ void for_each_vertex(const GraphDev& g, const HriBufs& h, F f) {
   const long long nt = (long long)gridDim.x * blockDim.x;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (!h.ranges) {
-    for (long long v = t; v < g.n; v += nt) classify_one(g, h, st, (int)v);
-    if (h.bmF) {
-      const long long words = ((long long)g.n + 31) / 32 + 1;
-      for (long long w = t; w < words; w += nt) h.bmF[w] = 0u;
-    }
+    for (long long v = t; v < g.n; v += nt) f((int)v);
     return;
   }
-  // the ranges' vertices, as one index space (binary search for the range)
   const int cnt = h.ranges[0];
   const long long total = h.ranges[1];
   const int* r = h.ranges + 2;  // (first vertex, vertices before) per range
@@ -60,9 +52,55 @@ __global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
       const int mid = (lo + hi + 1) / 2;
       if ((long long)r[2 * mid + 1] <= x) lo = mid; else hi = mid - 1;
     }
-    const int v = r[2 * lo] + (int)(x - r[2 * lo + 1]);
-    classify_one(g, h, st, v);
-    if (h.bmF) atomicAnd(&h.bmF[v >> 5], ~(1u << (v & 31)));
+    f(r[2 * lo] + (int)(x - r[2 * lo + 1]));
+  }
+}
+
+// Rows with at least min_live live slots, counted per length class.
+__global__ void hri_count_kernel(GraphDev g, HriBufs h) {
+  __shared__ unsigned s_cnt[32];
+  if (threadIdx.x < 32) s_cnt[threadIdx.x] = 0u;
+  __syncthreads();
+  for_each_vertex(g, h, [&](int v) {
+    const int L = g.live[v];
+    if (L >= h.min_live) atomicAdd(&s_cnt[len_class(L)], 1u);
+  });
+  __syncthreads();
+  if (threadIdx.x < 32 && s_cnt[threadIdx.x] != 0u)
+    atomicAdd(&h.bcnt[threadIdx.x], (unsigned long long)s_cnt[threadIdx.x]);
+}
+
+// Index i of every such row, class by class from the longest (so when the
+// copies outgrow their buffer, the rows that lose their index are the
+// shortest), in arrival order within a class; clears the changed-colour
+// bitmap of the covered vertices.
+__global__ void hri_classify_kernel(GraphDev g, HriBufs h, DevState* st) {
+  __shared__ unsigned long long s_base[32];
+  if (threadIdx.x < 32) {
+    unsigned long long b = 0;
+    for (int c = 31; c > (int)threadIdx.x; --c) b += h.bcnt[c];
+    s_base[threadIdx.x] = b;
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->hcount = b + h.bcnt[0];
+  }
+  __syncthreads();
+  for_each_vertex(g, h, [&](int v) {
+    int id = -1;
+    const int L = g.live[v];
+    if (L >= h.min_live) {
+      const int c = len_class(L);
+      const unsigned long long i = s_base[c] + atomicAdd(&h.bcnt[32 + c], 1ull);
+      if ((long long)i < h.cap_rows) {
+        id = (int)i;
+        h.hrow[i] = v;
+      }
+    }
+    h.hid[v] = id;
+    if (h.bmF && h.ranges) atomicAnd(&h.bmF[v >> 5], ~(1u << (v & 31)));
+  });
+  if (h.bmF && !h.ranges) {
+    const long long nt = (long long)gridDim.x * blockDim.x;
+    const long long words = ((long long)g.n + 31) / 32 + 1;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += nt) h.bmF[w] = 0u;
   }
 }
 
@@ -222,6 +260,9 @@ cudaError_t launch_hri_build(const GraphDev& g, const HriBufs& h, DevState* st, 
   long long b = ((long long)g.n + kHriThreads - 1) / kHriThreads;
   if (b > 148 * 16) b = 148 * 16;
   if (b < 1) b = 1;
+  cudaError_t e = cudaMemsetAsync(h.bcnt, 0, 64 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  hri_count_kernel<<<(unsigned)b, kHriThreads, 0, s>>>(g, h);
   hri_classify_kernel<<<(unsigned)b, kHriThreads, 0, s>>>(g, h, st);
   hri_offsets_kernel<<<1, kHriThreads, 0, s>>>(g, h, st);
   if (variant == DC_HB)

@@ -81,7 +81,7 @@ struct DevState {
   unsigned long long t_struct[2];     // %globaltimer at the start and end of the structural launch
   unsigned long long t_recolor[2];    // same for the recolour launch
   unsigned long long phase_ns[6];     // recolour launch: seeding, find-eligible, mex, commit, 2 spare
-  // heavy-row index (HI)
+  // heavy-row index
   unsigned long long hcount;          // rows found with at least min_live live slots
   unsigned long long a_count;         // (vertex, chunk) items waiting for the append phase
   unsigned hri_off;                   // 1: the index is incomplete for this batch; full scans only
@@ -146,14 +146,14 @@ struct StructParams {
   DevState* st;
 };
 
-// Heavy-row index (HI only).  Per batch, every row with at least
-// `min_live` live slots gets a copy of its neighbours ordered by their colour
-// at the start of the recolour launch (descending), and a list of its
-// neighbours whose colour has changed since.  findEligibleNeighbors marks a
-// neighbour u of v only if color[u] > prev[v] or color[u] == color[v], so
-// for such a row it reads the head of the ordered copy, the segment of
-// colour color[v], and the list, instead of gathering every neighbour's
-// colour.
+// Heavy-row index.  Per batch, every row with at least `min_live` live
+// slots gets a copy of its neighbours.  HI: ordered by their colour at the
+// start of the recolour launch (descending), and a list of its neighbours
+// whose colour has changed since.  HB: its neighbours prior to it first.
+// HI's findEligibleNeighbors marks a neighbour u of v only if
+// color[u] > prev[v] or color[u] == color[v], so for such a row it reads
+// the head of the ordered copy, the segment of colour color[v], and the
+// list, instead of gathering every neighbour's colour.
 constexpr int kHeavyMinLive = 2048;   // HI
 constexpr int kHeavyMinLiveHB = 256;  // HB: its index only splits rows by priority, cheap to build
 // A batch uses the index when lines * kIndexBatchRatio >= n.
@@ -174,6 +174,7 @@ struct HriBufs {
                               // that have not changed colour since (the append phase takes them off)
   int* hsplit;                // HB, cap_rows: row i's copy (in ids) holds its prior neighbours first,
                               // hsplit[i] of them, then the rest
+  unsigned long long* bcnt;   // 64: rows per length class, then the classes' cursors (build scratch)
   long long cap_rows, cap_pairs, cap_exc, cap_a, cap_hist;
   int min_live;               // 0: no index
   // Vertex ranges the index covers (nullptr: every vertex): [count, total,

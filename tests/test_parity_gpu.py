@@ -311,13 +311,16 @@ def test_greedy_initial_colouring_of_the_resident_graph():
 
 
 @pytest.mark.parametrize("variant,ov", VARIANTS)
-@pytest.mark.parametrize("min_live,unit_slots", [(64, 128), (256, 2048), (-1, 2048)])
+@pytest.mark.parametrize("min_live,unit_slots", [(64, 128), (256, 2048), (-1, 2048), (4, 128)])
 def test_heavy_row_index_matches_oracle(variant, ov, min_live, unit_slots):
     """The per-batch index of heavy rows (HI: neighbours ordered by colour
     plus change lists; HB: prior neighbours first) with many rows indexed,
     rows split over many units, and the index off: colours, iterations,
     frontier sizes and covered entries stay those of the oracle, while the
-    entries actually read drop when the index is on."""
+    entries actually read drop when the index is on.  From 4 live slots the
+    rows' copies outgrow the copy buffer (a quarter of the pool's slots for
+    HI, half for HB), so the shortest rows lose their index and are
+    scanned."""
     n, a, b = rmat_graph(14, 16, seed=5)
     col = dc.greedy_color(n, a, b)
     es = dc.EdgeSet(n, a, b)
